@@ -1,0 +1,85 @@
+"""Builds fr_learn_b200/libfrgpu.so in-tree for sm_100a.
+
+    python -m fr_learn_b200.build            # incremental
+    python -m fr_learn_b200.build --force
+
+Host set-up code (csrc/setup.cpp) is compiled by g++ -O2 without -march so
+its floating-point arithmetic matches a plain x86-64 build of the reference;
+the CUDA sources are compiled by nvcc for sm_100a only.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libfrgpu.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC"] + ARCH
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
+
+CU_SOURCES = ["frgpu.cu"]
+CXX_SOURCES = ["setup.cpp"]
+HEADERS = ["kernels.cuh", "physics.cuh", "setup.h"]
+
+
+def _nvcc():
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    p = os.path.join(cuda, "bin", "nvcc")
+    return p if os.path.exists(p) else shutil.which("nvcc")
+
+
+def _cxx():
+    for c in ("/usr/bin/g++", shutil.which("g++")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("no g++ found")
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} {os.path.basename(cmd[-1])}")
+    return r
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "frgpu.h")]
+    objs = []
+    for src in CXX_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        if force or _newer(o, [s] + hdrs):
+            _run([_cxx()] + CXX_FLAGS + ["-c", s, "-o", o])
+        objs.append(o)
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        if force or _newer(o, [s] + hdrs):
+            r = _run([_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o])
+            if verbose:
+                sys.stderr.write(r.stderr)
+        objs.append(o)
+    if force or _newer(LIB, objs):
+        _run([_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,894 @@
+// frgpu.cu -- the C ABI (include/frgpu.h): handle, device buffers, kernel
+// dispatch over (dimension, order, fields, precision), the RK driver and its
+// CUDA-graph replay.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/frgpu.h"
+#include "kernels.cuh"
+#include "setup.h"
+
+namespace frg {
+
+// ----------------------------------------------------------------- kernels
+__global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__restrict__ dA,
+                             const double *__restrict__ vol, const double *__restrict__ wsurf, int NF, int NFF,
+                             int nE, double cflFac, double *eleDt, double *blockMin, unsigned *ticket,
+                             double *dtOut, unsigned *err) {
+  __shared__ double wmin[32];
+  __shared__ bool last;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double my = INFINITY;
+  if (e < nE) {
+    double iw = 0;
+    for (int f = 0; f < NF; f++) iw += waveSp[(size_t)f * nE + e] * wsurf[f % NFF] * dA[(size_t)f * nE + e];
+    double dte = cflFac * vol[e] / iw;  // (CFL * limit * 2) * vol / intWave
+    eleDt[e] = dte;
+    my = dte;
+  }
+  // NaN must win the minimum so that it is detected
+  for (int o = 16; o > 0; o >>= 1) {
+    double t = __shfl_xor_sync(0xffffffffu, my, o);
+    my = (isnan(t) || t < my) ? t : my;
+  }
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = my;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? wmin[threadIdx.x] : INFINITY;
+    for (int o = 16; o > 0; o >>= 1) {
+      double t = __shfl_xor_sync(0xffffffffu, v, o);
+      v = (isnan(t) || t < v) ? t : v;
+    }
+    if (threadIdx.x == 0) {
+      blockMin[blockIdx.x] = v;
+      __threadfence();
+      last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (!last) return;
+  double v = INFINITY;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    double t = ((volatile double *)blockMin)[b];
+    v = (isnan(t) || t < v) ? t : v;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = (isnan(t) || t < v) ? t : v;
+  }
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = INFINITY;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = (isnan(wmin[w]) || wmin[w] < r) ? wmin[w] : r;
+    *dtOut = r;
+    if (isnan(r) || r < 1e-13) atomicOr(err, ERRF_DT);
+    *ticket = 0;
+  }
+}
+
+__global__ void fr_timestep_kernel(double *U, const double *U0, const double *divF, const double *detJ,
+                                   const double *dt, int dtLocal, double coef, int modeB, int NS, int nE,
+                                   long total) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const long pe = i % ((long)NS * nE);
+  const int e = (int)(pe % nE);
+  const double dtl = dtLocal ? dt[e] : dt[0];
+  if (modeB) U[i] -= coef * divF[i] / detJ[pe] * dtl;
+  else U[i] = U0[i] - coef * divF[i] / detJ[pe] * dtl;
+}
+
+__global__ void fr_norm_kernel(const double *divF, const double *detJ, const double *wvol, int NV, int NS, int nE,
+                               int normType, double *partial, unsigned *ticket, double *out) {
+  // one thread per element: its per-field norm (spt order as the reference),
+  // then per-block totals over elements in index order
+  extern __shared__ double sh[];  // [blockDim][NV]
+  __shared__ bool last;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int v = 0; v < NV; v++) {
+    double r = 0;
+    if (e < nE)
+      for (int s = 0; s < NS; s++) {
+        double dv = divF[((size_t)v * NS + s) * nE + e], dj = detJ[(size_t)s * nE + e];
+        if (normType == 1) r += fabs(dv) * wvol[s];
+        else if (normType == 2) r += dv * dv / dj * wvol[s];
+        else r = fmax(fabs(dv) / dj, r);
+      }
+    sh[threadIdx.x * NV + v] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int v = 0; v < NV; v++) {
+      double t = 0;
+      for (int i = 0; i < (int)blockDim.x; i++)
+        t = normType == 3 ? fmax(t, sh[i * NV + v]) : t + sh[i * NV + v];
+      partial[(size_t)blockIdx.x * NV + v] = t;
+    }
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  for (int v = 0; v < NV; v++) {
+    double t = 0;
+    for (int b = 0; b < (int)gridDim.x; b++) {
+      double x = ((volatile double *)partial)[(size_t)b * NV + v];
+      t = normType == 3 ? fmax(t, x) : t + x;
+    }
+    out[v] = t;
+  }
+  *ticket = 0;
+}
+
+__global__ void fr_to_device_layout(const double *ref, double *dev, int NV, int NPT, int nE) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // ref index
+  const long total = (long)NV * NPT * nE;
+  if (i >= total) return;
+  const int v = (int)(i % NV);
+  const long pe = i / NV;  // pt * nE + e
+  dev[(long)v * NPT * nE + pe] = ref[i];
+}
+__global__ void fr_to_ref_layout(const double *dev, double *ref, int NV, int NPT, int nE) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // ref index
+  const long total = (long)NV * NPT * nE;
+  if (i >= total) return;
+  const int v = (int)(i % NV);
+  const long pe = i / NV;
+  ref[i] = dev[(long)v * NPT * nE + pe];
+}
+template <typename S>
+__global__ void fr_cast_kernel(const double *in, S *out, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (S)in[i];
+}
+
+// ------------------------------------------------------------ dispatch table
+struct KernelSet {
+  void (*stage)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
+  void (*trace)(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) = nullptr;
+  void (*wavesp)(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph,
+                 cudaStream_t st) = nullptr;
+  int TE = 0;
+  size_t smem = 0;
+};
+
+template <class C, typename R, typename S>
+void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
+  fr_stage_kernel<C, R, S><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
+}
+template <class C, typename R, typename S>
+void launch_trace(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) {
+  long n = (long)C::NF * nE;
+  fr_trace_kernel<C, R, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U, static_cast<S *>(tr), nE, vcjh);
+}
+template <int DIM, int NV, typename S>
+void launch_wavesp(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph, cudaStream_t st) {
+  long n = (long)NF * nE;
+  fr_wavesp_kernel<DIM, NV, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<const S *>(tr), nrmOwn, ws,
+                                                                             NF, nE, ph);
+}
+
+template <int DIM, int P, int NV, typename R, typename S>
+bool make_set(KernelSet &k, std::string &err) {
+  using C = Cfg<DIM, P, NV>;
+  using T = Tile<C, R>;
+  k.stage = &launch_stage<C, R, S>;
+  k.trace = &launch_trace<C, R, S>;
+  k.wavesp = &launch_wavesp<DIM, NV, S>;
+  k.TE = T::TE;
+  k.smem = T::SMEM;
+  cudaError_t e = cudaFuncSetAttribute(fr_stage_kernel<C, R, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)T::SMEM);
+  if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+template <int DIM, int NV, typename R, typename S>
+bool select_order(int P, KernelSet &k, std::string &err) {
+  switch (P) {
+    case 1: return make_set<DIM, 1, NV, R, S>(k, err);
+    case 2: return make_set<DIM, 2, NV, R, S>(k, err);
+    case 3: return make_set<DIM, 3, NV, R, S>(k, err);
+    case 4: return make_set<DIM, 4, NV, R, S>(k, err);
+    case 5:
+      if constexpr (DIM == 2) return make_set<DIM, 5, NV, R, S>(k, err);
+      break;
+  }
+  err = "order not available for this dimension (2D: 1..5, 3D: 1..4)";
+  return false;
+}
+
+bool select_kernels(int nDims, int P, int NV, int prec, KernelSet &k, std::string &err) {
+  if (prec == FRG_FP64) {
+    if (nDims == 2 && NV == 1) return select_order<2, 1, double, double>(P, k, err);
+    if (nDims == 2 && NV == 4) return select_order<2, 4, double, double>(P, k, err);
+    if (nDims == 3 && NV == 1) return select_order<3, 1, double, double>(P, k, err);
+    if (nDims == 3 && NV == 5) return select_order<3, 5, double, double>(P, k, err);
+  } else {
+    if (nDims == 2 && NV == 1) return select_order<2, 1, float, float>(P, k, err);
+    if (nDims == 2 && NV == 4) return select_order<2, 4, float, float>(P, k, err);
+    if (nDims == 3 && NV == 1) return select_order<3, 1, float, float>(P, k, err);
+    if (nDims == 3 && NV == 5) return select_order<3, 5, float, float>(P, k, err);
+  }
+  err = "unsupported dimension / field count";
+  return false;
+}
+
+}  // namespace frg
+
+using namespace frg;
+
+// -------------------------------------------------------------- the handle
+struct frg_solver {
+  frg_params p{};
+  HostGeom g;
+  Ops1D ops;
+  KernelSet ks;
+  int nV = 0, nS = 0, nF = 0, nE = 0, nBlk = 0, nRK = 0;
+  size_t sstore = 8;  // bytes of the stored type
+  std::vector<double> RKa, RKb;
+  cudaStream_t stream = nullptr;
+  // device buffers
+  double *U = nullptr, *U0 = nullptr, *Acc = nullptr, *divF[5] = {nullptr};
+  void *W[2] = {nullptr, nullptr}, *tr[2] = {nullptr, nullptr};
+  void *nrm = nullptr, *dAs = nullptr, *JG = nullptr, *detJs = nullptr;
+  double *detJd = nullptr, *nrmOwn = nullptr, *dAd = nullptr, *vol = nullptr, *wsurf = nullptr, *wvol = nullptr;
+  int *nbr = nullptr;
+  double *waveSp = nullptr, *eleDt = nullptr, *dtDev = nullptr, *timeDev = nullptr, *blockMin = nullptr;
+  double *normPartial = nullptr, *normOut = nullptr, *scratchRef = nullptr;
+  unsigned *err = nullptr, *ticket = nullptr;
+  int curTr = 0;
+  bool trValid = false, divF0Valid = false, monitor = false;
+  int iter = 0, initIter = 0;
+  long long launches = 0;
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [firstIter][curTr]
+};
+
+namespace {
+thread_local std::string g_err;
+bool g_tables = false;
+
+frg_status fail(frg_status st, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return st;
+}
+#define CK(x)                                                                                    \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess) return fail(FRG_ERR_CUDA, "%s: %s (%s:%d)", #x, cudaGetErrorString(e_), \
+                                       __FILE__, __LINE__);                                      \
+  } while (0)
+
+frg_status upload_tables() {
+  if (g_tables) return FRG_OK;
+  static OpTab<double> hd[4][KMAXP + 1];
+  static OpTab<float> hf[4][KMAXP + 1];
+  for (int sch = 0; sch < 4; sch++)
+    for (int P = 0; P <= KMAXP; P++) {
+      if (sch == 3 && P < 2) continue;  // C+ is tabulated for P = 2..5 only
+      if (sch == 2 && P == 0) continue;
+      Ops1D o = build_ops1d(P, sch);
+      OpTab<double> &d = hd[sch][P];
+      OpTab<float> &f = hf[sch][P];
+      for (int i = 0; i <= KMAXP; i++) {
+        d.lag[0][i] = o.lag[0][i]; d.lag[1][i] = o.lag[1][i];
+        d.gL[i] = o.gL[i]; d.gR[i] = o.gR[i]; d.w[i] = o.w[i];
+        f.lag[0][i] = (float)o.lag[0][i]; f.lag[1][i] = (float)o.lag[1][i];
+        f.gL[i] = (float)o.gL[i]; f.gR[i] = (float)o.gR[i]; f.w[i] = (float)o.w[i];
+        for (int j = 0; j <= KMAXP; j++) { d.dlag[i][j] = o.dlag[i][j]; f.dlag[i][j] = (float)o.dlag[i][j]; }
+      }
+    }
+  CK(cudaMemcpyToSymbol(c_opd, hd, sizeof hd));
+  CK(cudaMemcpyToSymbol(c_opf, hf, sizeof hf));
+  g_tables = true;
+  return FRG_OK;
+}
+
+Phys make_phys(const frg_params &p) {
+  Phys ph{};
+  ph.gamma = p.gamma;
+  ph.adv[0] = p.advectVx; ph.adv[1] = p.advectVy; ph.adv[2] = p.advectVz;
+  ph.lambda = p.lambda;
+  ph.rhoB = p.rhoBound; ph.vB[0] = p.uBound; ph.vB[1] = p.vBound; ph.vB[2] = p.wBound; ph.pB = p.pBound;
+  ph.mu = p.mu_inf; ph.prandtl = p.prandtl; ph.c_sth = p.c_sth; ph.rt_inf = p.rt_inf;
+  ph.penFact = p.penFact; ph.tau = p.tau;
+  ph.TWall = p.TWall; ph.RGas = p.RGas; ph.vWall[0] = p.uWall; ph.vWall[1] = p.vWall; ph.vWall[2] = p.wWall;
+  ph.fixVis = p.fixVis;
+  ph.riemann = p.riemannType;
+  return ph;
+}
+
+template <typename T>
+frg_status dalloc(T **ptr, size_t count) {
+  CK(cudaMalloc((void **)ptr, count * sizeof(T) + 16));
+  CK(cudaMemset(*ptr, 0, count * sizeof(T) + 16));
+  return FRG_OK;
+}
+frg_status dalloc_bytes(void **ptr, size_t bytes) {
+  CK(cudaMalloc(ptr, bytes + 16));
+  CK(cudaMemset(*ptr, 0, bytes + 16));
+  return FRG_OK;
+}
+// copy a double host array to device in the stored precision
+frg_status upload_store(frg_solver *s, void **dst, const std::vector<double> &src) {
+  frg_status st = dalloc_bytes(dst, src.size() * s->sstore);
+  if (st) return st;
+  if (s->sstore == 8) {
+    CK(cudaMemcpy(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(src.begin(), src.end());
+    CK(cudaMemcpy(*dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+  }
+  return FRG_OK;
+}
+frg_status upload_d(double **dst, const std::vector<double> &src) {
+  frg_status st = dalloc(dst, src.size());
+  if (st) return st;
+  CK(cudaMemcpy(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+  return FRG_OK;
+}
+
+frg_status post_launch(frg_solver *s) {
+  s->launches++;
+  CK(cudaGetLastError());
+  return FRG_OK;
+}
+
+frg_status ensure_traces(frg_solver *s) {
+  if (s->trValid) return FRG_OK;
+  s->ks.trace(s->U, s->tr[s->curTr], s->nE, s->p.vcjhScheme, s->stream);
+  frg_status st = post_launch(s);
+  if (st) return st;
+  s->trValid = true;
+  return FRG_OK;
+}
+
+StageArgs base_args(frg_solver *s) {
+  StageArgs a{};
+  a.nE = s->nE;
+  a.nbr = s->nbr;
+  a.nrm = s->nrm;
+  a.dA = s->dAs;
+  a.JG = s->JG;
+  a.detJ = s->detJs;
+  a.waveSp = s->waveSp;
+  a.dt = s->p.dtType == 2 ? s->eleDt : s->dtDev;
+  a.dtLocal = s->p.dtType == 2;
+  a.time = s->timeDev;
+  a.err = s->err;
+  a.vcjh = s->p.vcjhScheme;
+  a.ph = make_phys(s->p);
+  return a;
+}
+
+frg_status launch_stage_args(frg_solver *s, StageArgs &a) {
+  s->ks.stage(&a, s->nBlk, s->ks.smem, s->stream);
+  return post_launch(s);
+}
+
+// getCFLLimit (src/global.cpp:45-66)
+const double kCflLimit[6] = {1.393, 0.464, 0.235, 0.1453, 0.100, 0.0736};
+
+frg_status launch_dt(frg_solver *s) {
+  int nb = (s->nE + 255) / 256;
+  double fac = s->p.CFL * kCflLimit[s->p.order] * 2;
+  fr_dt_kernel<<<nb, 256, 0, s->stream>>>(s->waveSp, s->dAd, s->vol, s->wsurf, s->nF, s->g.nFF, s->nE, fac,
+                                           s->eleDt, s->blockMin, s->ticket, s->dtDev, s->err);
+  return post_launch(s);
+}
+
+frg_status launch_wavesp(frg_solver *s) {
+  s->ks.wavesp(s->tr[s->curTr], s->nrmOwn, s->waveSp, s->nF, s->nE, make_phys(s->p), s->stream);
+  return post_launch(s);
+}
+
+// One fused step (the body of solver::update) on the stream.
+frg_status enqueue_step(frg_solver *s, bool firstIter) {
+  frg_status st;
+  if (s->p.dtType != 0) {
+    if (firstIter && (st = launch_wavesp(s))) return st;
+    if ((st = launch_dt(s))) return st;
+  }
+  const int nRK = s->nRK;
+  const bool jam = s->p.timeType == 5;
+  for (int k = 0; k < nRK; k++) {
+    StageArgs a = base_args(s);
+    const bool first = k == 0, last = k == nRK - 1;
+    a.Uin_d = first ? s->U : nullptr;
+    a.Uin_s = first ? nullptr : s->W[(k - 1) & 1];
+    a.U0 = s->U;
+    a.Acc = s->Acc;
+    a.Uout = s->U;
+    a.Wout = s->W[k & 1];
+    a.trIn = s->tr[s->curTr];
+    a.trOut = s->tr[s->curTr ^ 1];
+    a.aNext = jam ? s->RKa[k + 1] : (last ? 0.0 : s->RKa[k + 1]);
+    a.bCur = jam ? 0.0 : s->RKb[k];
+    a.flags = (last ? SF_WAVESP | SF_LAST | SF_TIME : 0) | (first ? SF_FIRST : 0) | (jam ? SF_JAMESON : 0);
+    if (first && s->monitor) {
+      a.flags |= SF_DIVF;
+      a.divF = s->divF[0];
+    }
+    if ((st = launch_stage_args(s, a))) return st;
+    s->curTr ^= 1;
+  }
+  return FRG_OK;
+}
+
+frg_status check_flags(frg_solver *s) {
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, s->err, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (h) {
+    CK(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->stream));
+    if (h & ERRF_NAN) return fail(FRG_ERR_NAN, "NaN encountered in the solution");
+    if (h & ERRF_DT) return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
+    if (h & ERRF_BC) return fail(FRG_ERR_ARG, "Boundary condition not recognized");
+  }
+  return FRG_OK;
+}
+
+frg_status unfused_update(frg_solver *s);
+
+}  // namespace
+
+// ==================================================================== C ABI
+extern "C" {
+
+const char *frg_last_error(void) { return g_err.c_str(); }
+const char *frg_version(void) { return "frgpu 0.1 sm_100a"; }
+
+frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver **out) {
+  if (!params || !mesh || !out || !mesh->xv || !mesh->c2v) return fail(FRG_ERR_ARG, "null argument");
+  *out = nullptr;
+  const frg_params &p = *params;
+  if (p.nDims != 2 && p.nDims != 3) return fail(FRG_ERR_ARG, "nDims must be 2 or 3");
+  if (p.order < 1 || p.order > (p.nDims == 2 ? 5 : 4)) return fail(FRG_ERR_ARG, "order %d not supported", p.order);
+  if (p.equation != 0 && p.equation != 1) return fail(FRG_ERR_ARG, "equation must be 0 or 1");
+  if (p.viscous) return fail(FRG_ERR_ARG, "viscous path not built yet");
+  if (p.equation == 1 && p.riemannType == 1 && p.nDims == 3)
+    return fail(FRG_ERR_ARG, "Roe not implemented in 3D");
+  if (p.vcjhScheme < 0 || p.vcjhScheme > 3 || (p.vcjhScheme == 3 && p.order < 2))
+    return fail(FRG_ERR_ARG, "invalid VCJH scheme");
+  if (p.precision != FRG_FP64 && p.precision != FRG_MIXED) return fail(FRG_ERR_ARG, "invalid precision");
+  if (p.dtType < 0 || p.dtType > 2) return fail(FRG_ERR_ARG, "invalid dtType");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(FRG_ERR_CUDA, "no CUDA device");
+  std::unique_ptr<frg_solver> s(new frg_solver());
+  s->p = p;
+  s->nV = p.equation == 0 ? 1 : p.nDims + 2;
+  switch (p.timeType) {
+    case 0: s->nRK = 1; s->RKa = {0}; s->RKb = {1}; break;
+    case 2: s->nRK = 2; s->RKa = {0, 1.}; s->RKb = {1. / 2., 1. / 2.}; break;
+    case 4: s->nRK = 4; s->RKa = {0., .5, .5, 1.}; s->RKb = {1. / 6., 1. / 3., 1. / 3., 1. / 6.}; break;
+    case 5: s->nRK = 4; s->RKa = {0., 1. / 4., 1. / 3., 1. / 2., 1.0}; s->RKb = {0.}; break;
+    default: return fail(FRG_ERR_ARG, "Time-Stepping type not supported.");
+  }
+  std::string err;
+  frg_status st = build_geometry(p, *mesh, s->g, err);
+  if (st) return fail(st, "%s", err.c_str());
+  s->ops = build_ops1d(p.order, p.vcjhScheme);
+  s->nS = s->g.nS; s->nF = s->g.nF; s->nE = s->g.nE;
+  if ((st = upload_tables())) return st;
+  if (!select_kernels(p.nDims, p.order, s->nV, p.precision, s->ks, err)) return fail(FRG_ERR_ARG, "%s", err.c_str());
+  s->sstore = p.precision == FRG_FP64 ? 8 : 4;
+  s->nBlk = (s->nE + s->ks.TE - 1) / s->ks.TE;
+  CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  const size_t nSE = (size_t)s->nV * s->nS * s->nE, nFE = (size_t)s->nV * s->nF * s->nE;
+  if ((st = dalloc(&s->U, nSE)) || (st = dalloc(&s->U0, nSE)) || (st = dalloc(&s->Acc, nSE))) return st;
+  for (int i = 0; i < 2; i++) {
+    if ((st = dalloc_bytes(&s->W[i], nSE * s->sstore))) return st;
+    if ((st = dalloc_bytes(&s->tr[i], nFE * s->sstore))) return st;
+  }
+  if ((st = upload_store(s.get(), &s->nrm, s->g.nrmC)) || (st = upload_store(s.get(), &s->dAs, s->g.dA)) ||
+      (st = upload_store(s.get(), &s->JG, s->g.JG)) || (st = upload_store(s.get(), &s->detJs, s->g.detJ)))
+    return st;
+  if ((st = upload_d(&s->detJd, s->g.detJ)) || (st = upload_d(&s->nrmOwn, s->g.nrmOwn)) ||
+      (st = upload_d(&s->dAd, s->g.dA)) || (st = upload_d(&s->vol, s->g.vol)))
+    return st;
+  {
+    std::vector<double> ws(s->g.nFF), wv(s->nS);
+    const int n1 = p.order + 1;
+    for (int k = 0; k < s->g.nFF; k++) ws[k] = p.nDims == 2 ? s->ops.w[k] : s->ops.w[k / n1] * s->ops.w[k % n1];
+    for (int q = 0; q < s->nS; q++) {
+      int i = q % n1, j = (q / n1) % n1, k = q / (n1 * n1);
+      wv[q] = p.nDims == 2 ? s->ops.w[j] * s->ops.w[i] : s->ops.w[k] * s->ops.w[j] * s->ops.w[i];
+    }
+    if ((st = upload_d(&s->wsurf, ws)) || (st = upload_d(&s->wvol, wv))) return st;
+  }
+  CK(cudaMalloc(&s->nbr, s->g.nbr.size() * sizeof(int)));
+  CK(cudaMemcpy(s->nbr, s->g.nbr.data(), s->g.nbr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  const int nbDt = (s->nE + 255) / 256;
+  if ((st = dalloc(&s->waveSp, (size_t)s->nF * s->nE)) || (st = dalloc(&s->eleDt, (size_t)s->nE)) ||
+      (st = dalloc(&s->dtDev, 1)) || (st = dalloc(&s->timeDev, 1)) || (st = dalloc(&s->blockMin, (size_t)nbDt)) ||
+      (st = dalloc(&s->normPartial, (size_t)nbDt * s->nV)) || (st = dalloc(&s->normOut, (size_t)s->nV)) ||
+      (st = dalloc(&s->err, 1)) || (st = dalloc(&s->ticket, 1)))
+    return st;
+  if (p.dtType == 0) CK(cudaMemcpy(s->dtDev, &p.dt, sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaDeviceSynchronize());
+  *out = s.release();
+  return FRG_OK;
+}
+
+frg_status frg_inspect_geometry(const frg_params *params, const frg_mesh *mesh, int which, double *out,
+                                long *count) {
+  if (!params || !mesh || !count) return fail(FRG_ERR_ARG, "null argument");
+  HostGeom g;
+  std::string err;
+  frg_status st = build_geometry(*params, *mesh, g, err);
+  if (st) return fail(st, "%s", err.c_str());
+  const int d = g.nDims, nS = g.nS, nF = g.nF, nE = g.nE;
+  std::vector<double> r;
+  switch (which) {
+    case 0: r = g.pos_spts; break;
+    case 1:
+      r.resize(g.JG.size());
+      for (int a = 0; a < d; a++)
+        for (int b = 0; b < d; b++)
+          for (int q = 0; q < nS; q++)
+            for (int e = 0; e < nE; e++)
+              r[(((size_t)a * nS + q) * nE + e) * d + b] = g.JG[(((size_t)a * d + b) * nS + q) * nE + e];
+      break;
+    case 2: r = g.detJ; break;
+    case 3:
+      r.resize(g.nrmOwn.size());
+      for (int k = 0; k < d; k++)
+        for (int f = 0; f < nF; f++)
+          for (int e = 0; e < nE; e++) r[((size_t)f * nE + e) * d + k] = g.nrmOwn[((size_t)k * nF + f) * nE + e];
+      break;
+    case 4: r = g.dA; break;
+    case 5: r.assign(g.faceTable.begin(), g.faceTable.end()); break;
+    default: return fail(FRG_ERR_ARG, "unknown geometry item %d", which);
+  }
+  *count = (long)r.size();
+  if (out) std::memcpy(out, r.data(), r.size() * sizeof(double));
+  return FRG_OK;
+}
+
+frg_status frg_destroy(frg_solver *s) {
+  if (!s) return FRG_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto &r : s->graph)
+    for (auto &g : r)
+      if (g) cudaGraphExecDestroy(g);
+  double *dp[] = {s->U, s->U0, s->Acc, s->divF[0], s->divF[1], s->divF[2], s->divF[3], s->divF[4], s->detJd,
+                  s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
+                  s->blockMin, s->normPartial, s->normOut, s->scratchRef};
+  for (double *q : dp) if (q) cudaFree(q);
+  void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->nbr, s->err, s->ticket};
+  for (void *q : vp) if (q) cudaFree(q);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return FRG_OK;
+}
+
+frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, int *nEles) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  if (nSpts) *nSpts = s->nS;
+  if (nFpts) *nFpts = s->nF;
+  if (nFields) *nFields = s->nV;
+  if (nEles) *nEles = s->nE;
+  return FRG_OK;
+}
+
+frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out) {
+  if (!s || !out || which < 0 || which > 4 || dim < 0 || dim >= s->p.nDims) return fail(FRG_ERR_ARG, "bad operator request");
+  std::vector<double> m;
+  dense_operator(s->p.nDims, s->ops, which, dim, m);
+  std::memcpy(out, m.data(), m.size() * sizeof(double));
+  return FRG_OK;
+}
+
+static frg_status ref_scratch(frg_solver *s, size_t n) {
+  if (!s->scratchRef) {
+    size_t big = (size_t)s->nV * std::max(s->nS, s->nF) * s->nE;
+    frg_status st = dalloc(&s->scratchRef, big);
+    if (st) return st;
+  }
+  (void)n;
+  return FRG_OK;
+}
+
+frg_status frg_upload(frg_solver *s, int array, const double *host) {
+  if (!s || !host) return fail(FRG_ERR_ARG, "null argument");
+  if (array != FRG_U_SPTS && array != FRG_U0) return fail(FRG_ERR_ARG, "array not uploadable");
+  frg_status st = ref_scratch(s, 0);
+  if (st) return st;
+  const size_t n = (size_t)s->nV * s->nS * s->nE;
+  CK(cudaMemcpyAsync(s->scratchRef, host, n * 8, cudaMemcpyHostToDevice, s->stream));
+  fr_to_device_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->scratchRef,
+                                                                         array == FRG_U0 ? s->U0 : s->U, s->nV,
+                                                                         s->nS, s->nE);
+  if ((st = post_launch(s))) return st;
+  if (array == FRG_U_SPTS) s->trValid = false;
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
+frg_status frg_download(frg_solver *s, int array, int stage, double *host) {
+  if (!s || !host) return fail(FRG_ERR_ARG, "null argument");
+  frg_status st = ref_scratch(s, 0);
+  if (st) return st;
+  const double *src = nullptr;
+  int npt = s->nS;
+  switch (array) {
+    case FRG_U_SPTS: src = s->U; break;
+    case FRG_U0: src = s->U0; break;
+    case FRG_DIVF:
+      if (stage < 0 || stage >= s->nRK || !s->divF[stage]) return fail(FRG_ERR_ARG, "divF stage %d not computed", stage);
+      src = s->divF[stage];
+      break;
+    case FRG_U_FPTS: {
+      if ((st = ensure_traces(s))) return st;
+      npt = s->nF;
+      const size_t n = (size_t)s->nV * s->nF * s->nE;
+      if (s->sstore == 8) {
+        src = (const double *)s->tr[s->curTr];
+      } else {
+        // widen float traces on the host
+        std::vector<float> f(n);
+        CK(cudaMemcpyAsync(f.data(), s->tr[s->curTr], n * 4, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        for (int v = 0; v < s->nV; v++)
+          for (int q = 0; q < s->nF; q++)
+            for (int e = 0; e < s->nE; e++)
+              host[((size_t)q * s->nE + e) * s->nV + v] = f[((size_t)v * s->nF + q) * s->nE + e];
+        return FRG_OK;
+      }
+      break;
+    }
+    case FRG_POS_SPTS:
+      std::memcpy(host, s->g.pos_spts.data(), s->g.pos_spts.size() * 8);
+      return FRG_OK;
+    case FRG_DETJAC:
+      std::memcpy(host, s->g.detJ.data(), s->g.detJ.size() * 8);
+      return FRG_OK;
+    case FRG_WAVESP: {
+      std::vector<double> w((size_t)s->nF * s->nE);
+      CK(cudaMemcpyAsync(w.data(), s->waveSp, w.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      for (int f = 0; f < s->nF; f++)
+        for (int e = 0; e < s->nE; e++) host[(size_t)e * s->nF + f] = w[(size_t)f * s->nE + e];
+      return FRG_OK;
+    }
+    case FRG_ELE_DT:
+      CK(cudaMemcpyAsync(host, s->eleDt, (size_t)s->nE * 8, cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      return FRG_OK;
+    default:
+      return fail(FRG_ERR_ARG, "unknown array %d", array);
+  }
+  const size_t n = (size_t)s->nV * npt * s->nE;
+  fr_to_ref_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(src, s->scratchRef, s->nV, npt, s->nE);
+  if ((st = post_launch(s))) return st;
+  CK(cudaMemcpyAsync(host, s->scratchRef, n * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
+frg_status frg_set_initial_condition(frg_solver *s, int icType, double a0) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  std::vector<double> U;
+  std::string err;
+  frg_status st = initial_condition(s->p, s->g, icType, a0, U, err);
+  if (st) return fail(st, "%s", err.c_str());
+  return frg_upload(s, FRG_U_SPTS, U.data());
+}
+
+frg_status frg_calc_residual(frg_solver *s, int step) {
+  if (!s || step < 0 || step >= s->nRK) return fail(FRG_ERR_ARG, "bad step");
+  frg_status st;
+  if (!s->divF[step] && (st = dalloc(&s->divF[step], (size_t)s->nV * s->nS * s->nE))) return st;
+  // solver::extrapolateU always recomputes the traces of U_spts
+  s->trValid = false;
+  if ((st = ensure_traces(s))) return st;
+  StageArgs a = base_args(s);
+  a.Uin_d = s->U;
+  a.trIn = s->tr[s->curTr];
+  a.divF = s->divF[step];
+  a.flags = SF_RESIDUAL | SF_WAVESP;
+  if ((st = launch_stage_args(s, a))) return st;
+  if (step == 0) s->divF0Valid = true;
+  return FRG_OK;
+}
+
+frg_status frg_time_step_a(frg_solver *s, int step, double rkval) {
+  if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
+  const long n = (long)s->nV * s->nS * s->nE;
+  fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
+      s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev, s->p.dtType == 2, rkval, 0,
+      s->nS, s->nE, n);
+  s->trValid = false;
+  return post_launch(s);
+}
+
+frg_status frg_time_step_b(frg_solver *s, int step) {
+  if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
+  const long n = (long)s->nV * s->nS * s->nE;
+  fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
+      s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev, s->p.dtType == 2,
+      s->RKb[step], 1, s->nS, s->nE, n);
+  s->trValid = false;
+  return post_launch(s);
+}
+
+frg_status frg_copy_u_to_u0(frg_solver *s) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  CK(cudaMemcpyAsync(s->U0, s->U, (size_t)s->nV * s->nS * s->nE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  return FRG_OK;
+}
+frg_status frg_copy_u0_to_u(frg_solver *s) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  CK(cudaMemcpyAsync(s->U, s->U0, (size_t)s->nV * s->nS * s->nE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  s->trValid = false;
+  return FRG_OK;
+}
+
+frg_status frg_calc_dt(frg_solver *s, double *dt_out) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  frg_status st;
+  if (s->p.dtType != 0) {
+    if (s->iter == s->initIter + 1) {
+      // calcWaveSpFpts reads U_fpts as the last extrapolation left it
+      if ((st = ensure_traces(s)) || (st = launch_wavesp(s))) return st;
+    }
+    if ((st = launch_dt(s))) return st;
+  }
+  if ((st = check_flags(s))) return st;
+  if (dt_out) {
+    CK(cudaMemcpyAsync(dt_out, s->dtDev, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return FRG_OK;
+}
+
+frg_status frg_update(frg_solver *s, int nsteps) {
+  if (!s || nsteps < 0) return fail(FRG_ERR_ARG, "bad arguments");
+  frg_status st;
+  if (s->p.timeType == 0 && s->p.dtType != 0) {
+    // Forward Euler takes its CFL dt after the residual (src/solver.cpp:238-241):
+    // the reference's unfused sequence
+    for (int n = 0; n < nsteps; n++)
+      if ((st = unfused_update(s))) return st;
+    return check_flags(s);
+  }
+  if ((st = ensure_traces(s))) return st;
+  for (int n = 0; n < nsteps; n++) {
+    s->iter++;
+    const int fi = (s->p.dtType != 0 && s->iter == s->initIter + 1) ? 1 : 0;
+    const int ct = s->curTr;
+    cudaGraphExec_t &ge = s->graph[fi][ct];
+    if (!ge) {
+      cudaGraph_t gr;
+      long long before = s->launches;
+      CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      st = enqueue_step(s, fi);
+      cudaError_t ce = cudaStreamEndCapture(s->stream, &gr);
+      if (st) return st;
+      if (ce != cudaSuccess) return fail(FRG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      CK(cudaGraphInstantiate(&ge, gr, 0));
+      CK(cudaGraphDestroy(gr));
+      s->launches = before;
+      s->curTr = ct;
+    }
+    CK(cudaGraphLaunch(ge, s->stream));
+    // count the kernels the graph holds
+    s->launches += s->nRK + (s->p.dtType != 0 ? 1 + fi : 0);
+    s->curTr ^= (s->nRK & 1);
+  }
+  if (nsteps > 0) s->divF0Valid = s->monitor;
+  return check_flags(s);
+}
+
+frg_status frg_update_host(frg_solver *s, double *U_host, int nsteps) {
+  frg_status st = frg_upload(s, FRG_U_SPTS, U_host);
+  if (st) return st;
+  if ((st = frg_update(s, nsteps))) return st;
+  return frg_download(s, FRG_U_SPTS, 0, U_host);
+}
+
+frg_status frg_residual_norm(frg_solver *s, int normType, double *out) {
+  if (!s || !out || normType < 1 || normType > 3) return fail(FRG_ERR_ARG, "bad arguments");
+  if (!s->divF0Valid) return fail(FRG_ERR_ARG, "no stage-0 residual stored (call frg_calc_residual(0))");
+  const int nb = (s->nE + 255) / 256;
+  fr_norm_kernel<<<nb, 256, 256 * s->nV * sizeof(double), s->stream>>>(s->divF[0], s->detJd, s->wvol, s->nV, s->nS,
+                                                                        s->nE, normType, s->normPartial, s->ticket,
+                                                                        s->normOut);
+  frg_status st = post_launch(s);
+  if (st) return st;
+  CK(cudaMemcpyAsync(out, s->normOut, (size_t)s->nV * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
+frg_status frg_set_monitor(frg_solver *s, int enable) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  if ((enable != 0) == s->monitor) return FRG_OK;
+  s->monitor = enable != 0;
+  if (s->monitor && !s->divF[0]) {
+    frg_status st = dalloc(&s->divF[0], (size_t)s->nV * s->nS * s->nE);
+    if (st) return st;
+  }
+  // the captured steps carry the old flags
+  CK(cudaStreamSynchronize(s->stream));
+  for (auto &r : s->graph)
+    for (auto &g : r)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return FRG_OK;
+}
+
+frg_status frg_get_time(const frg_solver *s, double *time, double *dt, int *iter) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  if (time) { CK(cudaMemcpyAsync(time, s->timeDev, 8, cudaMemcpyDeviceToHost, s->stream)); }
+  if (dt) { CK(cudaMemcpyAsync(dt, s->dtDev, 8, cudaMemcpyDeviceToHost, s->stream)); }
+  CK(cudaStreamSynchronize(s->stream));
+  if (iter) *iter = s->iter;
+  return FRG_OK;
+}
+
+frg_status frg_set_iter(frg_solver *s, int iter, int initIter) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  s->iter = iter;
+  s->initIter = initIter;
+  return FRG_OK;
+}
+
+frg_status frg_sync(frg_solver *s) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
+frg_status frg_launch_count(const frg_solver *s, long long *count) {
+  if (!s || !count) return fail(FRG_ERR_ARG, "null argument");
+  *count = s->launches;
+  return FRG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// solver::update exactly as written (src/solver.cpp:212-250), on the device,
+// one kernel per reference call.
+frg_status unfused_update(frg_solver *s) {
+  frg_status st;
+  s->iter++;
+  const int nRK = s->nRK;
+  for (int step = 0; step < nRK - 1; step++) {
+    if (step == 0 && s->p.dtType != 0 && (st = frg_calc_dt(s, nullptr))) return st;
+    if (step == 0 && (st = frg_copy_u_to_u0(s))) return st;
+    if ((st = frg_calc_residual(s, step)) || (st = frg_time_step_a(s, step, s->RKa[step + 1]))) return st;
+  }
+  if ((st = frg_calc_residual(s, nRK - 1))) return st;
+  if (s->p.timeType < 5) {
+    if (nRK > 1) { if ((st = frg_copy_u0_to_u(s))) return st; }
+    else if (s->p.dtType != 0 && (st = frg_calc_dt(s, nullptr))) return st;
+    for (int step = 0; step < nRK; step++)
+      if ((st = frg_time_step_b(s, step))) return st;
+  } else {
+    if ((st = frg_time_step_a(s, nRK - 1, s->RKa[nRK]))) return st;
+  }
+  // time += dt
+  double t = 0, dt = 0;
+  CK(cudaMemcpyAsync(&t, s->timeDev, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(&dt, s->dtDev, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  t += dt;
+  CK(cudaMemcpyAsync(s->timeDev, &t, 8, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+}  // namespace

@@ -1,0 +1,262 @@
+// physics.cuh -- pointwise physics of the FR path as device functions:
+// inviscid fluxes, the Rusanov / Roe / Lax-Friedrichs common fluxes, boundary
+// ghost states and the viscous flux.  Each keeps the operation order of the
+// reference routine it restates (cited per function), so the FP64 build agrees
+// with the reference to rounding (FMA contraction aside).
+//
+// Template parameter R is the arithmetic type (double, or float in the mixed
+// mode); PR is the type of the Riemann solvers' pressure recovery
+// p = (gamma-1)(E - rho|v|^2/2), which is always double: at low Mach number E
+// and the kinetic energy nearly cancel.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace frg {
+
+// Parameters of the physics, as `input` holds them (include/input.hpp).
+struct Phys {
+  double gamma;
+  double adv[3];  // advectVx, advectVy, advectVz
+  double lambda;  // Lax-Friedrichs upwinding factor
+  double rhoB, vB[3], pB;
+  double mu, prandtl, c_sth, rt_inf;
+  double penFact, tau;
+  double TWall, RGas, vWall[3];
+  int fixVis;
+  int riemann;  // 0 Rusanov, 1 Roe
+};
+
+// BC_TYPE values (include/global.hpp:63-78)
+enum : int {
+  BC_CHAR = 1, BC_SUP_IN = 2, BC_SUP_OUT = 3, BC_SUB_IN = 4, BC_SUB_OUT = 5,
+  BC_SLIP = 8, BC_ISO_NOSLIP = 9, BC_ADI_NOSLIP = 10, BC_SYMMETRY = 12, BC_ISO_NOSLIP_MOVING = 13
+};
+
+// inviscidFlux (src/flux.cpp:37-88).  F[d][k]: flux of field k along x_d.
+template <int DIM, int NV, typename R>
+__device__ __forceinline__ void inviscid_flux(const R *U, R F[DIM][NV], const Phys &ph) {
+  if constexpr (NV == 1) {
+    F[0][0] = (R)ph.adv[0] * U[0];
+    F[1][0] = (R)ph.adv[1] * U[0];
+    if constexpr (DIM == 3) F[2][0] = (R)ph.adv[2] * U[0];
+  } else if constexpr (DIM == 2) {
+    const R g = (R)ph.gamma;
+    R rho = U[0], u = U[1] / rho, v = U[2] / rho, E = U[3];
+    R p = (g - (R)1.0) * (E - (R)0.5 * rho * (u * u + v * v));
+    F[0][0] = rho * u; F[1][0] = rho * v;
+    F[0][1] = rho * u * u + p; F[1][1] = rho * u * v;
+    F[0][2] = rho * v * u; F[1][2] = rho * v * v + p;
+    F[0][3] = (E + p) * u; F[1][3] = (E + p) * v;
+  } else {
+    const R g = (R)ph.gamma;
+    R rho = U[0], u = U[1] / rho, v = U[2] / rho, w = U[3] / rho, E = U[4];
+    R p = (g - (R)1.0) * (E - (R)0.5 * rho * (u * u + v * v + w * w));
+    F[0][0] = rho * u; F[1][0] = rho * v; F[2][0] = rho * w;
+    F[0][1] = rho * u * u + p; F[1][1] = rho * u * v; F[2][1] = rho * u * w;
+    F[0][2] = rho * v * u; F[1][2] = rho * v * v + p; F[2][2] = rho * v * w;
+    F[0][3] = rho * w * u; F[1][3] = rho * w * v; F[2][3] = rho * w * w + p;
+    F[0][4] = (E + p) * u; F[1][4] = (E + p) * v; F[2][4] = (E + p) * w;
+  }
+}
+
+// face::rusanovFlux, one flux point (src/face.cpp:289-356).  Returns the wave
+// speed max(|vn_L|+c_L, |vn_R|+c_R) that the reference stores for calcDt.
+template <int DIM, int NV, typename R, typename PR>
+__device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R *Fn, const Phys &ph) {
+  R FL[DIM][NV], FR[DIM][NV];
+  inviscid_flux<DIM, NV, R>(UL, FL, ph);
+  inviscid_flux<DIM, NV, R>(UR, FR, ph);
+  R FnL[NV], FnR[NV];
+#pragma unroll
+  for (int i = 0; i < NV; i++) { FnL[i] = 0; FnR[i] = 0; }
+  const PR g = (PR)ph.gamma;
+  PR rhoL = UL[0], rhoR = UR[0];
+  PR uL = (PR)UL[1] / rhoL, uR = (PR)UR[1] / rhoR, vL = (PR)UL[2] / rhoL, vR = (PR)UR[2] / rhoR;
+  PR pL, pR;
+  if constexpr (DIM == 2) {
+    pL = (g - (PR)1.0) * ((PR)UL[3] - (PR)0.5 * rhoL * (uL * uL + vL * vL));
+    pR = (g - (PR)1.0) * ((PR)UR[3] - (PR)0.5 * rhoR * (uR * uR + vR * vR));
+  } else {
+    PR wL = (PR)UL[3] / rhoL, wR = (PR)UR[3] / rhoR;
+    pL = (g - (PR)1.0) * ((PR)UL[4] - (PR)0.5 * rhoL * (uL * uL + vL * vL + wL * wL));
+    pR = (g - (PR)1.0) * ((PR)UR[4] - (PR)0.5 * rhoR * (uR * uR + vR * vR + wR * wR));
+  }
+  R vnL = 0, vnR = 0;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    vnL += n[d] * UL[d + 1] / UL[0];
+    vnR += n[d] * UR[d + 1] / UR[0];
+#pragma unroll
+    for (int i = 0; i < NV; i++) { FnL[i] += n[d] * FL[d][i]; FnR[i] += n[d] * FR[d][i]; }
+  }
+  R csqL = (R)fmax(g * pL / rhoL, (PR)0.0), csqR = (R)fmax(g * pR / rhoR, (PR)0.0);
+  R eigL = fabs(vnL) + sqrt(csqL), eigR = fabs(vnR) + sqrt(csqR);
+  R eig = eigL > eigR ? eigL : eigR;
+#pragma unroll
+  for (int i = 0; i < NV; i++) Fn[i] = (R)0.5 * (FnL[i] + FnR[i] - eig * (UR[i] - UL[i]));
+  return eig;
+}
+
+// face::roeFlux with the entropy fix, 2D (src/face.cpp:358-484).
+template <typename R, typename PR>
+__device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R *Fn, const Phys &ph) {
+  const R g = (R)ph.gamma;
+  R vL[2], vR[2], um[2], du[4];
+  for (int i = 0; i < 2; i++) { vL[i] = UL[i + 1] / UL[0]; vR[i] = UR[i + 1] / UR[0]; }
+  const PR gp = (PR)ph.gamma;
+  R pL = (R)((gp - (PR)1.0) * ((PR)UL[3] - ((PR)0.5 * (PR)UL[0] * ((PR)vL[0] * (PR)vL[0] + (PR)vL[1] * (PR)vL[1]))));
+  R pR = (R)((gp - (PR)1.0) * ((PR)UR[3] - ((PR)0.5 * (PR)UR[0] * ((PR)vR[0] * (PR)vR[0] + (PR)vR[1] * (PR)vR[1]))));
+  R hL = (UL[3] + pL) / UL[0], hR = (UR[3] + pR) / UR[0];
+  R sq_rho = sqrt(UR[0] / UL[0]);
+  R rrho = (R)1. / (sq_rho + (R)1.);
+  R usq = 0, unm = 0;
+  for (int i = 0; i < 2; i++) {
+    um[i] = rrho * (vL[i] + sq_rho * vR[i]);
+    usq += (R)0.5 * um[i] * um[i];
+    unm += um[i] * n[i];
+  }
+  R hm = rrho * (hL + sq_rho * hR);
+  R am_sq = (g - (R)1.) * (hm - usq);
+  R am = sqrt(am_sq);
+  R rhoUnL = 0, rhoUnR = 0;
+  for (int i = 0; i < 2; i++) { rhoUnL += UL[i + 1] * n[i]; rhoUnR += UR[i + 1] * n[i]; }
+  Fn[0] = rhoUnL + rhoUnR;
+  Fn[1] = rhoUnL * vL[0] + rhoUnR * vR[0] + (pL + pR) * n[0];
+  Fn[2] = rhoUnL * vL[1] + rhoUnR * vR[1] + (pL + pR) * n[1];
+  Fn[3] = rhoUnL * hL + rhoUnR * hR;
+  for (int i = 0; i < 4; i++) du[i] = UR[i] - UL[i];
+  R lambda0 = fabs(unm), lambdaP = fabs(unm + am), lambdaM = fabs(unm - am);
+  R eps = (R)0.5 * (fabs(rhoUnL / UL[0] - rhoUnR / UR[0]) + fabs(sqrt(g * pL / UL[0]) - sqrt(g * pR / UR[0])));
+  if (lambda0 < (R)2. * eps) lambda0 = (R)0.25 * lambda0 * lambda0 / eps + eps;
+  if (lambdaP < (R)2. * eps) lambdaP = (R)0.25 * lambdaP * lambdaP / eps + eps;
+  if (lambdaM < (R)2. * eps) lambdaM = (R)0.25 * lambdaM * lambdaM / eps + eps;
+  R a2 = (R)0.5 * (lambdaP + lambdaM) - lambda0;
+  R a3 = (R)0.5 * (lambdaP - lambdaM) / am;
+  R a1 = a2 * (g - (R)1.) / am_sq;
+  R a4 = a3 * (g - (R)1.);
+  R a5 = usq * du[0] - um[0] * du[1] - um[1] * du[2] + du[3];
+  R a6 = unm * du[0] - n[0] * du[1] - n[1] * du[2];
+  R aL1 = a1 * a5 - a3 * a6, bL1 = a4 * a5 - a2 * a6;
+  Fn[0] -= lambda0 * du[0] + aL1;
+  Fn[1] -= lambda0 * du[1] + aL1 * um[0] + bL1 * n[0];
+  Fn[2] -= lambda0 * du[2] + aL1 * um[1] + bL1 * n[1];
+  Fn[3] -= lambda0 * du[3] + aL1 * hm + bL1 * unm;
+  for (int i = 0; i < 4; i++) Fn[i] *= (R)0.5;
+}
+
+// face::laxFriedrichsFlux for scalar advection (src/face.cpp:486-514).
+template <int DIM, typename R>
+__device__ __forceinline__ R lax_friedrichs(R uL, R uR, const R *n, R *Fn, const Phys &ph) {
+  R uAvg = (R)0.5 * (uL + uR), uDiff = uL - uR;
+  R vN = (R)ph.adv[0] * n[0] + (R)ph.adv[1] * n[1];
+  if constexpr (DIM == 3) vN += (R)ph.adv[2] * n[2];
+  Fn[0] = vN * uAvg + (R)0.5 * (R)ph.lambda * fabs(vN) * uDiff;
+  return fabs(vN);
+}
+
+// boundFace::applyBCs for Euler/Navier-Stokes (src/boundFace.cpp:33-277),
+// computed in double.  Returns false for an unknown BC.
+template <int DIM>
+__device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, const Phys &ph) {
+  double rhoR = 0, pR = 0, ER = 0;
+  double vL[3] = {0, 0, 0}, vR[3] = {0, 0, 0};
+  const double gamma = ph.gamma, gmo = gamma - 1.;
+  double rhoL = UL[0], eL = UL[DIM + 1];
+  for (int i = 0; i < DIM; i++) vL[i] = UL[i + 1] / UL[0];
+  double vSq = 0;
+  for (int i = 0; i < DIM; i++) vSq += (vL[i] * vL[i]);
+  double pL = (gamma - 1.0) * (eL - 0.5 * rhoL * vSq);
+  switch (bc) {
+    case BC_SUB_IN:
+      rhoR = ph.rhoB;
+      for (int i = 0; i < DIM; i++) vR[i] = ph.vB[i];
+      pR = pL;
+      vSq = 0;
+      for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
+      ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
+      break;
+    case BC_SUB_OUT:
+      rhoR = rhoL;
+      for (int i = 0; i < DIM; i++) vR[i] = vL[i];
+      pR = ph.pB;
+      vSq = 0.;
+      for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
+      ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
+      break;
+    case BC_SUP_IN:
+      rhoR = ph.rhoB;
+      vR[0] = ph.vB[0]; vR[1] = ph.vB[1]; vR[2] = ph.vB[2];
+      pR = ph.pB;
+      vSq = 0.;
+      for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
+      ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
+      break;
+    case BC_SUP_OUT:
+      rhoR = rhoL;
+      for (int i = 0; i < DIM; i++) vR[i] = vL[i];
+      ER = eL;
+      break;
+    case BC_SLIP:
+    case BC_SYMMETRY: {
+      rhoR = rhoL;
+      double vnL = 0.;
+      for (int i = 0; i < DIM; i++) vnL += (vL[i] - 0.0) * n[i];
+      for (int i = 0; i < DIM; i++) vR[i] = vL[i] - (2.0) * vnL * n[i];
+      ER = eL;
+      break;
+    }
+    case BC_ISO_NOSLIP_MOVING:
+    case BC_ISO_NOSLIP: {
+      pR = pL;
+      rhoR = pR / (ph.RGas * ph.TWall);
+      for (int i = 0; i < DIM; i++) vR[i] = bc == BC_ISO_NOSLIP_MOVING ? 0.0 + ph.vWall[i] : 0.0;
+      vSq = 0.;
+      for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
+      ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
+      break;
+    }
+    case BC_ADI_NOSLIP:
+      rhoR = rhoL;
+      pR = pL;
+      for (int i = 0; i < DIM; i++) vR[i] = 0.0;
+      vSq = 0.;
+      for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
+      ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
+      break;
+    case BC_CHAR: {
+      double vnL = 0., vnB = 0.;
+      for (int i = 0; i < DIM; i++) vnL += vL[i] * n[i];
+      for (int i = 0; i < DIM; i++) vnB += ph.vB[i] * n[i];
+      double cL = sqrt(gamma * pL / rhoL);
+      double cB = sqrt(gamma * ph.pB / ph.rhoB);
+      double R_L, R_B;
+      if (fabs(vnB) >= cB && vnL >= 0) R_L = vnB + 2. / gmo * cB;
+      else R_L = vnL + 2. / gmo * cL;
+      if (fabs(vnB) >= cB && vnL < 0) R_B = vnL - 2. / gmo * cL;
+      else R_B = vnB - 2. / gmo * cB;
+      double rhoFac = .25 * (gamma - 1.) * (R_L - R_B);
+      double rhoBG = rhoFac * rhoFac / gamma;
+      if (vnL < 0) rhoBG *= pow(ph.rhoB, gamma) / ph.pB;
+      else rhoBG *= pow(rhoL, gamma) / pL;
+      rhoR = pow(rhoBG, 1. / gmo);
+      pR = rhoFac * rhoFac * rhoR / gamma;
+      double VB = 0.5 * (R_L + R_B);
+      for (int i = 0; i < DIM; i++) {
+        if (vnL < 0) vR[i] = ph.vB[i] + (VB - vnB) * n[i];
+        else vR[i] = vL[i] + (VB - vnL) * n[i];
+      }
+      double vMag2 = 0;
+      for (int i = 0; i < DIM; i++) vMag2 += vR[i] * vR[i];
+      ER = pR / gmo + .5 * rhoR * vMag2;
+      break;
+    }
+    default:
+      return false;
+  }
+  UR[0] = rhoR;
+  for (int i = 0; i < DIM; i++) UR[i + 1] = rhoR * vR[i];
+  UR[DIM + 1] = ER;
+  return true;
+}
+
+}  // namespace frg

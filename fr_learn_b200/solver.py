@@ -1,0 +1,260 @@
+"""Python mirror of FlurryPP's solver entry points over the libfrgpu C ABI.
+
+Method names follow the reference's `solver` (include/solver.hpp:137-153):
+``calcResidual``, ``update``, ``timeStepA``, ``timeStepB``, ``copyUspts_U0``,
+``copyU0_Uspts``, ``calcDt``, plus ``getNormResidual`` (writeResidual's sum of
+ele::getNormResidual) and the ``input`` parameter names.  Arrays cross the
+boundary in the reference's layouts ([point][element][field]).
+
+There is no CPU fallback: importing works without a GPU, but creating a
+Solver raises if libfrgpu.so is missing or no CUDA device is usable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .mesh import Mesh
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfrgpu.so")
+
+FRG_FP64, FRG_MIXED = 0, 1
+ARRAYS = {"U_spts": 0, "U0": 1, "divF_spts": 2, "U_fpts": 3, "pos_spts": 4, "waveSp": 5, "detJac_spts": 6,
+          "ele_dt": 7}
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NAN", 4: "ERR_NEG_JAC", 5: "ERR_DT", 6: "ERR_TIMEOUT",
+          7: "ERR_MESH"}
+
+
+class FrgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nDims", C.c_int), ("order", C.c_int), ("equation", C.c_int), ("viscous", C.c_int),
+        ("riemannType", C.c_int), ("vcjhScheme", C.c_int), ("timeType", C.c_int), ("dtType", C.c_int),
+        ("dt", C.c_double), ("CFL", C.c_double), ("gamma", C.c_double),
+        ("advectVx", C.c_double), ("advectVy", C.c_double), ("advectVz", C.c_double),
+        ("lambda_", C.c_double), ("diffD", C.c_double),
+        ("rhoBound", C.c_double), ("uBound", C.c_double), ("vBound", C.c_double),
+        ("wBound", C.c_double), ("pBound", C.c_double),
+        ("mu_inf", C.c_double), ("prandtl", C.c_double), ("c_sth", C.c_double), ("rt_inf", C.c_double),
+        ("fixVis", C.c_int), ("penFact", C.c_double), ("tau", C.c_double),
+        ("TWall", C.c_double), ("RGas", C.c_double), ("uWall", C.c_double), ("vWall", C.c_double),
+        ("wWall", C.c_double), ("precision", C.c_int),
+    ]
+
+
+class MeshC(C.Structure):
+    _fields_ = [("nEles", C.c_int), ("nNodes", C.c_int), ("xv", C.c_void_p), ("c2v", C.c_void_p),
+                ("bc", C.c_void_p)]
+
+
+def default_params(**kw) -> dict:
+    """Defaults of input::readInputFile (src/input.cpp:214-475)."""
+    d = dict(nDims=2, order=3, equation=1, viscous=0, riemannType=0, vcjhScheme=0, timeType=4, dtType=0,
+             dt=1e-3, CFL=0.5, gamma=1.4, advectVx=1.0, advectVy=1.0, advectVz=0.0, lambda_=1.0, diffD=1.0,
+             rhoBound=1.0, uBound=0.2, vBound=0.0, wBound=0.0, pBound=0.7142857143,
+             mu_inf=1.0 / 1600.0, prandtl=0.72, c_sth=0.0, rt_inf=1.0, fixVis=1, penFact=0.0, tau=1.0,
+             TWall=1.0, RGas=1.0, uWall=0.0, vWall=0.0, wWall=0.0, precision=FRG_FP64)
+    if "lambda" in kw:
+        kw["lambda_"] = kw.pop("lambda")
+    d.update(kw)
+    return d
+
+
+_lib = None
+
+
+def lib():
+    """Loads libfrgpu.so (building it if this is a source checkout without it)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _b
+        _b.build()
+    L = C.CDLL(LIB_PATH)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    sig = {
+        "frg_last_error": ([], C.c_char_p), "frg_version": ([], C.c_char_p),
+        "frg_create": ([C.POINTER(Params), C.POINTER(MeshC), C.POINTER(vp)], i),
+        "frg_destroy": ([vp], i),
+        "frg_info": ([vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)], i),
+        "frg_get_operator": ([vp, i, i, vp], i),
+        "frg_upload": ([vp, i, vp], i), "frg_download": ([vp, i, i, vp], i),
+        "frg_set_initial_condition": ([vp, i, d], i),
+        "frg_calc_residual": ([vp, i], i), "frg_time_step_a": ([vp, i, d], i), "frg_time_step_b": ([vp, i], i),
+        "frg_copy_u_to_u0": ([vp], i), "frg_copy_u0_to_u": ([vp], i),
+        "frg_calc_dt": ([vp, C.POINTER(d)], i), "frg_update": ([vp, i], i), "frg_update_host": ([vp, vp, i], i),
+        "frg_residual_norm": ([vp, i, vp], i), "frg_set_monitor": ([vp, i], i),
+        "frg_get_time": ([vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)], i),
+        "frg_set_iter": ([vp, i, i], i), "frg_sync": ([vp], i),
+        "frg_launch_count": ([vp, C.POINTER(C.c_longlong)], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(code):
+    if code != 0:
+        raise FrgError(code, lib().frg_last_error().decode())
+
+
+class Solver:
+    """One FR solver on the current CUDA device (a drop-in for `solver`)."""
+
+    def __init__(self, mesh: Mesh, **params):
+        self.params = default_params(nDims=mesh.nDims, **params)
+        self.mesh = mesh
+        L = lib()
+        p = Params(**self.params)
+        xv = np.ascontiguousarray(mesh.xv, np.float64)
+        c2v = np.ascontiguousarray(mesh.c2v, np.int32)
+        bc = np.ascontiguousarray(mesh.bc, np.int32)
+        m = MeshC(mesh.nEles, mesh.nNodes, xv.ctypes.data, c2v.ctypes.data, bc.ctypes.data)
+        h = C.c_void_p()
+        _check(L.frg_create(C.byref(p), C.byref(m), C.byref(h)))
+        self.h = h
+        nS, nF, nV, nE = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(L.frg_info(h, C.byref(nS), C.byref(nF), C.byref(nV), C.byref(nE)))
+        self.nSpts, self.nFpts, self.nFields, self.nEles = nS.value, nF.value, nV.value, nE.value
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            lib().frg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- data
+    def _shape(self, name):
+        nS, nF, nV, nE, d = self.nSpts, self.nFpts, self.nFields, self.nEles, self.params["nDims"]
+        return {"U_spts": (nS, nE, nV), "U0": (nS, nE, nV), "divF_spts": (nS, nE, nV), "U_fpts": (nF, nE, nV),
+                "pos_spts": (nS, nE, d), "waveSp": (nE, nF), "detJac_spts": (nS, nE), "ele_dt": (nE,)}[name]
+
+    def get(self, name, stage=0):
+        out = np.empty(self._shape(name), np.float64)
+        _check(lib().frg_download(self.h, ARRAYS[name], stage, out.ctypes.data))
+        return out
+
+    def set(self, name, arr):
+        a = np.ascontiguousarray(arr, np.float64)
+        assert a.shape == self._shape(name), (a.shape, self._shape(name))
+        _check(lib().frg_upload(self.h, ARRAYS[name], a.ctypes.data))
+
+    def operator(self, which, dim=0):
+        nS, nF = self.nSpts, self.nFpts
+        shape = {0: (nF, nS), 1: (nS, nS), 2: (nF, nS), 3: (nS, nF), 4: (nS, nF)}[which]
+        out = np.empty(shape, np.float64)
+        _check(lib().frg_get_operator(self.h, which, dim, out.ctypes.data))
+        return out
+
+    # -- the reference's entry points
+    def setInitialCondition(self, icType=None, a0=0.0):
+        _check(lib().frg_set_initial_condition(self.h, self.params.get("icType", 1) if icType is None else icType, a0))
+
+    def calcResidual(self, step=0):
+        _check(lib().frg_calc_residual(self.h, step))
+
+    def timeStepA(self, step, RKval):
+        _check(lib().frg_time_step_a(self.h, step, RKval))
+
+    def timeStepB(self, step):
+        _check(lib().frg_time_step_b(self.h, step))
+
+    def copyUspts_U0(self):
+        _check(lib().frg_copy_u_to_u0(self.h))
+
+    def copyU0_Uspts(self):
+        _check(lib().frg_copy_u0_to_u(self.h))
+
+    def calcDt(self):
+        dt = C.c_double()
+        _check(lib().frg_calc_dt(self.h, C.byref(dt)))
+        return dt.value
+
+    def update(self, nsteps=1):
+        """nsteps iterations of the main loop body (iter++; solver::update())."""
+        _check(lib().frg_update(self.h, nsteps))
+
+    def update_host(self, U_host, nsteps=1):
+        _check(lib().frg_update_host(self.h, U_host.ctypes.data, nsteps))
+
+    def getNormResidual(self, normType=2):
+        out = np.empty(self.nFields, np.float64)
+        _check(lib().frg_residual_norm(self.h, normType, out.ctypes.data))
+        return out
+
+    def setMonitor(self, enable=True):
+        _check(lib().frg_set_monitor(self.h, int(enable)))
+
+    def setIter(self, it, initIter=0):
+        _check(lib().frg_set_iter(self.h, it, initIter))
+
+    @property
+    def time(self):
+        t, dt, it = C.c_double(), C.c_double(), C.c_int()
+        _check(lib().frg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(it)))
+        return t.value
+
+    @property
+    def dt(self):
+        t, dt, it = C.c_double(), C.c_double(), C.c_int()
+        _check(lib().frg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(it)))
+        return dt.value
+
+    @property
+    def iter(self):
+        t, dt, it = C.c_double(), C.c_double(), C.c_int()
+        _check(lib().frg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(it)))
+        return it.value
+
+    def sync(self):
+        _check(lib().frg_sync(self.h))
+
+    def launch_count(self):
+        n = C.c_longlong()
+        _check(lib().frg_launch_count(self.h, C.byref(n)))
+        return n.value
+
+
+def inspect_geometry(mesh: Mesh, which: str, **params) -> np.ndarray:
+    """Host-only: the metrics / face table frg_create would build (no GPU needed)."""
+    items = {"pos_spts": 0, "JGinv_spts": 1, "detJac_spts": 2, "norm_fpts": 3, "dA_fpts": 4, "faces": 5}
+    L = lib()
+    L.frg_inspect_geometry.argtypes = [C.POINTER(Params), C.POINTER(MeshC), C.c_int, C.c_void_p,
+                                       C.POINTER(C.c_long)]
+    L.frg_inspect_geometry.restype = C.c_int
+    p = Params(**default_params(nDims=mesh.nDims, **params))
+    xv = np.ascontiguousarray(mesh.xv, np.float64)
+    c2v = np.ascontiguousarray(mesh.c2v, np.int32)
+    bc = np.ascontiguousarray(mesh.bc, np.int32)
+    m = MeshC(mesh.nEles, mesh.nNodes, xv.ctypes.data, c2v.ctypes.data, bc.ctypes.data)
+    n = C.c_long()
+    _check(L.frg_inspect_geometry(C.byref(p), C.byref(m), items[which], None, C.byref(n)))
+    out = np.empty(n.value, np.float64)
+    _check(L.frg_inspect_geometry(C.byref(p), C.byref(m), items[which], out.ctypes.data, C.byref(n)))
+    if which == "faces":
+        return out.reshape(-1, 6).astype(np.int64)
+    return out

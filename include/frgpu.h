@@ -1,0 +1,172 @@
+/* frgpu.h -- C ABI of the B200 flux-reconstruction residual + Runge-Kutta path.
+ *
+ * Drop-in boundary for FlurryPP's solver entry points (include/solver.hpp:137-153
+ * of the reference):
+ *
+ *   solver::calcResidual(int step)              -> frg_calc_residual
+ *   solver::timeStepA(int step, double RKval)   -> frg_time_step_a
+ *   solver::timeStepB(int step)                 -> frg_time_step_b
+ *   solver::copyUspts_U0 / copyU0_Uspts         -> frg_copy_u_to_u0 / frg_copy_u0_to_u
+ *   solver::calcDt()                            -> frg_calc_dt
+ *   solver::update()  (+ the main loop's iter++,
+ *                      src/flurry.cpp:50-53)     -> frg_update
+ *   ele::getNormResidual summed as writeResidual
+ *     does (src/ele.cpp:1882, src/output.cpp:846) -> frg_residual_norm
+ *   oper::setupOperators(eType, order, ...)      -> built inside frg_create;
+ *     (src/operators.cpp:13)                        frg_get_operator returns the
+ *                                                   dense matrices for checking
+ *   ele::setInitialCondition (src/ele.cpp:683)   -> frg_set_initial_condition
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Every function returns an frg_status.
+ *   - Host arrays use the reference's layouts: solution [point][element][field]
+ *     (src/solver.cpp:65-107).  Device arrays are [field][point][element].
+ *   - Host buffers are caller-owned; device buffers are owned by the handle.
+ *   - A handle is not thread-safe: one CUDA stream, calls serialised by the
+ *     caller.  The reference is single-threaded too (makefile:14).
+ *   - Errors replace the reference's fatalError()+exit(1) (include/error.hpp:10):
+ *     the call returns a code and frg_last_error() gives the message.
+ *   - There is no CPU fallback: without a usable CUDA device frg_create fails.
+ */
+#ifndef FRGPU_H
+#define FRGPU_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum frg_status {
+  FRG_OK = 0,
+  FRG_ERR_ARG = 1,         /* invalid argument or unsupported configuration */
+  FRG_ERR_CUDA = 2,        /* CUDA runtime error, or no device */
+  FRG_ERR_NAN = 3,         /* NaN in the solution (src/output.cpp:833-841) */
+  FRG_ERR_NEG_JAC = 4,     /* negative Jacobian (src/solver.cpp:1283) */
+  FRG_ERR_DT = 5,          /* dt < 1e-13 (src/output.cpp:823-824) */
+  FRG_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
+  FRG_ERR_MESH = 7         /* unmatched face, self-neighbour, bad element */
+} frg_status;
+
+typedef enum frg_precision {
+  FRG_FP64 = 0,  /* everything in FP64 */
+  FRG_MIXED = 1  /* FP32 operators/fluxes/traces/metrics; FP64 Riemann pressure,
+                    RK accumulation and norms */
+} frg_precision;
+
+/* Input parameters, same names and meaning as the reference's `input`
+ * (include/input.hpp:63-234, src/input.cpp:214-554). Viscous runs take the
+ * already non-dimensionalised values (input::nonDimensionalize). */
+typedef struct frg_params {
+  int nDims;       /* 2 or 3 */
+  int order;       /* P: 1..5 in 2D, 1..4 in 3D */
+  int equation;    /* 0 advection, 1 Euler / Navier-Stokes */
+  int viscous;     /* 0 / 1 */
+  int riemannType; /* 0 Rusanov, 1 Roe (2D) */
+  int vcjhScheme;  /* 0 DG, 1 SD, 2 HU, 3 C+ */
+  int timeType;    /* 0 FE, 2 RK2, 4 RK44, 5 RK44 (Jameson form) */
+  int dtType;      /* 0 fixed, 1 global CFL, 2 local CFL */
+  double dt, CFL;
+  double gamma;
+  double advectVx, advectVy, advectVz, lambda, diffD;
+  double rhoBound, uBound, vBound, wBound, pBound;
+  double mu_inf, prandtl, c_sth, rt_inf;
+  int fixVis;
+  double penFact, tau;
+  double TWall, RGas, uWall, vWall, wWall;
+  int precision; /* frg_precision */
+} frg_params;
+
+/* Mesh: element node coordinates and the vertex ids used to pair faces.
+ * xv  [nEles][nNodes][nDims], node order of the reference's shape functions
+ *     (src/funcs.cpp:126, :183): quads of any Lagrange order (4, 9, 16, ...
+ *     nodes), 8-node hexahedra.
+ * c2v [nEles][nCorners] (4 or 8); periodic images share one id.
+ * bc  [nEles][nFacesPerEle] (4 or 6): reference BC_TYPE of a face on a
+ *     boundary (include/global.hpp:63-78), -1 for faces paired by c2v. */
+typedef struct frg_mesh {
+  int nEles;
+  int nNodes;
+  const double *xv;
+  const int *c2v;
+  const int *bc;
+} frg_mesh;
+
+typedef struct frg_solver frg_solver;
+
+/* which arrays frg_download / frg_upload address */
+typedef enum frg_array {
+  FRG_U_SPTS = 0,   /* [nSpts][nEles][nFields] current solution (solver::U_spts) */
+  FRG_U0 = 1,       /* [nSpts][nEles][nFields] (solver::U0) */
+  FRG_DIVF = 2,     /* [nSpts][nEles][nFields] divF_spts[stage] (reference space) */
+  FRG_U_FPTS = 3,   /* [nFpts][nEles][nFields] traces of the current solution */
+  FRG_POS_SPTS = 4, /* [nSpts][nEles][nDims] physical solution-point positions */
+  FRG_WAVESP = 5,   /* [nEles][nFpts] wave speeds kept for calcDt */
+  FRG_DETJAC = 6,   /* [nSpts][nEles] */
+  FRG_ELE_DT = 7    /* [nEles] per-element CFL dt of the last calcDt */
+} frg_array;
+
+const char *frg_last_error(void);
+const char *frg_version(void);
+
+/* Creates a solver on the current CUDA device: connectivity, metrics,
+ * operators (setup work, host side), device buffers.  Rejects configurations
+ * the reference rejects (3D Roe: src/face.cpp:362; negative Jacobian). */
+frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver **out);
+
+/* Host-only inspection of the set-up (no device needed): the metrics and
+ * connectivity frg_create would build, in the reference's layouts.
+ * which: 0 pos_spts [nS][nE][d], 1 JGinv_spts [d][nS][nE][d], 2 detJac_spts
+ * [nS][nE], 3 norm_fpts [nF][nE][d], 4 dA_fpts [nF][nE], 5 face table
+ * [nFaces][6] (eL, locF_L, eR, locF_R, relRot, bc) written as doubles.
+ * With out == NULL only *count is set. */
+frg_status frg_inspect_geometry(const frg_params *params, const frg_mesh *mesh, int which, double *out,
+                                long *count);
+frg_status frg_destroy(frg_solver *s);
+frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, int *nEles);
+
+/* Dense operator matrices, row-major, as oper::setupOperators builds them:
+ * which 0 opp_spts_to_fpts [nF][nS], 1 opp_grad_spts[dim] [nS][nS],
+ * 2 opp_extrapolateFn[dim] [nF][nS], 3 opp_correction [nS][nF],
+ * 4 opp_correctU[dim] [nS][nF]. */
+frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out);
+
+frg_status frg_upload(frg_solver *s, int array, const double *host);
+frg_status frg_download(frg_solver *s, int array, int stage, double *host);
+
+/* ele::setInitialCondition: icType 0 freestream / Gaussian, 1 isentropic
+ * vortex (eps 5) / sine, 2 Liang vortex; 10 Taylor-Green vortex (a0 = Mach);
+ * 11 isentropic vortex of strength a0 (eps generalised). */
+frg_status frg_set_initial_condition(frg_solver *s, int icType, double a0);
+
+/* solver::calcResidual(step): divF_spts[step] of the current solution. */
+frg_status frg_calc_residual(frg_solver *s, int step);
+frg_status frg_time_step_a(frg_solver *s, int step, double rkval);
+frg_status frg_time_step_b(frg_solver *s, int step);
+frg_status frg_copy_u_to_u0(frg_solver *s);
+frg_status frg_copy_u0_to_u(frg_solver *s);
+/* solver::calcDt: on the first iteration recomputes the wave speeds
+ * (ele::calcWaveSpFpts), then dt = min over elements (warp-shuffle reduction). */
+frg_status frg_calc_dt(frg_solver *s, double *dt_out);
+
+/* nsteps iterations of the reference main loop body (iter++; update()), as
+ * one fused kernel per RK stage replayed from a CUDA graph.  Device-resident:
+ * no host transfer.  Checks the NaN / dt flags after the last step. */
+frg_status frg_update(frg_solver *s, int nsteps);
+/* Same, with the solution in host memory ([spt][ele][field]): upload,
+ * nsteps iterations, download. */
+frg_status frg_update_host(frg_solver *s, double *U_host, int nsteps);
+
+/* writeResidual's norm of divF_spts[0] (normType 1, 2 or 3) of the last
+ * calcResidual(0) or, after frg_set_monitor(s, 1), of the last update. */
+frg_status frg_residual_norm(frg_solver *s, int normType, double *out /*[nFields]*/);
+frg_status frg_set_monitor(frg_solver *s, int enable);
+
+frg_status frg_get_time(const frg_solver *s, double *time, double *dt, int *iter);
+frg_status frg_set_iter(frg_solver *s, int iter, int initIter);
+/* Synchronise the handle's stream (all work finished). */
+frg_status frg_sync(frg_solver *s);
+/* Device-side launch counter: kernels launched by this handle so far. */
+frg_status frg_launch_count(const frg_solver *s, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

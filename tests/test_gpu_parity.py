@@ -1,0 +1,155 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+FP64 mode: the bar is 1e-12 relative (max-norm over the array, relative to
+the array's max) for a residual and for multi-step updates.  Mixed mode: the
+stated bound is checked in test_mixed_precision_bound.
+"""
+import numpy as np
+import pytest
+
+from conftest import relerr
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+
+
+def pair(oracle, mesh, ic, a0=0.0, **kw):
+    from fr_learn_b200 import Solver
+
+    g = Solver(mesh, **kw)
+    okw = {k: v for k, v in kw.items() if k != "precision"}
+    o = oracle.Oracle(oracle.params(nDims=mesh.nDims, **okw), mesh)
+    o.set_ic(ic, a0)
+    g.setInitialCondition(ic, a0)
+    assert relerr(g.get("U_spts"), o.U()) == 0.0
+    return g, o
+
+
+def cases():
+    from fr_learn_b200 import box2d, box3d, bump2d
+
+    char6 = {s: "char" for s in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")}
+    return {
+        "vortex2d_p4_roe": (box2d(8, 8, -10, 10, -10, 10, perturb=0.1, seed=7), 1,
+                            dict(order=4, riemannType=1, dtType=1, CFL=0.5)),
+        "vortex2d_p3_rusanov": (box2d(6, 7, -10, 10, -10, 10, perturb=0.1, seed=8), 1,
+                                dict(order=3, riemannType=0, dtType=0, dt=2e-3)),
+        "vortex2d_p5_roe": (box2d(5, 5, -10, 10, -10, 10, perturb=0.05, seed=9), 1,
+                            dict(order=5, riemannType=1, dtType=1, CFL=0.3)),
+        "advection2d_p3": (box2d(8, 8), 0, dict(order=3, equation=0, dt=1e-3)),
+        "advection2d_p2_cfl": (box2d(6, 5, perturb=0.1, seed=1), 0, dict(order=2, equation=0, dtType=1, CFL=0.5)),
+        "bump2d_p3_roe": (bump2d(12, 4), 0, dict(order=3, riemannType=1, dtType=1, CFL=0.5,
+                                                  uBound=0.5 * np.sqrt(1.4), pBound=1.0)),
+        "euler3d_p2_char": (box3d(3, 3, 3, (-2, -2, -2), (2, 2, 2), bcs=char6, perturb=0.1, seed=1), 1,
+                            dict(order=2, dtType=1, CFL=0.5)),
+        "euler3d_p3_periodic": (box3d(3, 3, 4, perturb=0.1, seed=2), 10,
+                                dict(order=3, dtType=0, dt=1e-3)),
+        "advection3d_p2": (box3d(3, 3, 3, (-2, -2, -2), (2, 2, 2), bcs=char6), 0,
+                           dict(order=2, equation=0, dtType=1, CFL=0.3)),
+    }
+
+
+CASES = list(cases().keys())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_residual_fp64(oracle, name):
+    mesh, ic, kw = cases()[name]
+    a0 = 0.1 if ic == 10 else 0.0
+    g, o = pair(oracle, mesh, ic, a0, **kw)
+    g.calcResidual(0)
+    o.calc_residual(0)
+    assert relerr(g.get("U_fpts"), o.get("U_fpts")) < FP64_TOL
+    assert relerr(g.get("divF_spts", 0), o.divF(0)) < FP64_TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_update_fp64(oracle, name):
+    mesh, ic, kw = cases()[name]
+    a0 = 0.1 if ic == 10 else 0.0
+    g, o = pair(oracle, mesh, ic, a0, **kw)
+    for _ in range(3):
+        g.update(1)
+        o.update(1)
+        assert relerr(g.dt, o.dt) < FP64_TOL
+    assert relerr(g.get("U_spts"), o.U()) < FP64_TOL
+    assert abs(g.time - o.time) <= 1e-12 * max(o.time, 1e-300) + 1e-300
+
+
+@pytest.mark.parametrize("timeType,dtType", [(0, 0), (0, 1), (2, 1), (5, 0), (4, 2)])
+def test_rk_variants(oracle, timeType, dtType):
+    from fr_learn_b200 import box2d
+
+    mesh = box2d(6, 6, -10, 10, -10, 10, perturb=0.1, seed=3)
+    g, o = pair(oracle, mesh, 1, order=3, riemannType=1, timeType=timeType, dtType=dtType, dt=1e-3, CFL=0.3)
+    g.update(3)
+    o.update(3)
+    assert relerr(g.get("U_spts"), o.U()) < FP64_TOL
+
+
+def test_unfused_entry_points_match_update(oracle):
+    """calcResidual/timeStepA/timeStepB driven by hand (solver::update's body)
+    equals the fused frg_update step."""
+    from fr_learn_b200 import Solver, box2d
+
+    mesh = box2d(6, 6, -10, 10, -10, 10, perturb=0.1, seed=4)
+    kw = dict(order=4, riemannType=1, dtType=0, dt=2e-3)
+    a, b = Solver(mesh, **kw), Solver(mesh, **kw)
+    a.setInitialCondition(1)
+    b.setInitialCondition(1)
+    a.update(1)
+    RKa, RKb = [0., .5, .5, 1.], [1 / 6, 1 / 3, 1 / 3, 1 / 6]
+    b.copyUspts_U0()
+    for s in range(3):
+        b.calcResidual(s)
+        b.timeStepA(s, RKa[s + 1])
+    b.calcResidual(3)
+    b.copyU0_Uspts()
+    for s in range(4):
+        b.timeStepB(s)
+    assert relerr(a.get("U_spts"), b.get("U_spts")) < FP64_TOL
+
+
+def test_residual_norm(oracle):
+    from fr_learn_b200 import box2d
+
+    mesh = box2d(6, 6, -10, 10, -10, 10, perturb=0.1, seed=5)
+    g, o = pair(oracle, mesh, 1, order=3, riemannType=1)
+    g.calcResidual(0)
+    o.calc_residual(0)
+    for t in (1, 2, 3):
+        assert relerr(g.getNormResidual(t), o.residual_norm(t)) < FP64_TOL
+    g.setMonitor(True)
+    g.update(2)
+    o.update(2)
+    assert relerr(g.getNormResidual(2), o.residual_norm(2)) < FP64_TOL
+
+
+def test_mixed_precision_bound(oracle):
+    """Mixed mode (FP32 operators, fluxes, traces, metrics; FP64 Riemann
+    pressure and RK accumulation) stays within 1e-5 relative of the FP64
+    oracle over 20 RK4 steps of the perturbed-mesh vortex."""
+    from fr_learn_b200 import FRG_MIXED, box2d
+
+    mesh = box2d(8, 8, -10, 10, -10, 10, perturb=0.1, seed=7)
+    g, o = pair(oracle, mesh, 1, order=4, riemannType=1, dtType=0, dt=5e-3, precision=FRG_MIXED)
+    g.update(20)
+    o.update(20)
+    U, R = g.get("U_spts"), o.U()
+    l2 = np.linalg.norm(U - R) / np.linalg.norm(R)
+    assert l2 < 1e-5, l2
+    assert relerr(U, R) < 1e-5
+
+
+def test_operators_match_oracle(oracle):
+    from fr_learn_b200 import Solver, box2d, box3d
+
+    for mesh, P in ((box2d(3, 3), 4), (box3d(3, 3, 3), 3)):
+        g = Solver(mesh, order=P)
+        o = oracle.Oracle(oracle.params(nDims=mesh.nDims, order=P), mesh)
+        assert np.array_equal(g.operator(0), o.get("opp_spts_to_fpts").reshape(g.nFpts, g.nSpts))
+        assert np.array_equal(g.operator(3), o.get("opp_correction").reshape(g.nSpts, g.nFpts))
+        for d in range(mesh.nDims):
+            assert np.array_equal(g.operator(1, d), o.get(f"opp_grad_spts{d}").reshape(g.nSpts, g.nSpts))
+            assert np.array_equal(g.operator(2, d), o.get(f"opp_extrapolateFn{d}").reshape(g.nFpts, g.nSpts))
