@@ -1,0 +1,363 @@
+"""Benchmark of the FR residual + RK4 path: DOF-updates/s on B200.
+
+Workload (default): 2D Euler isentropic vortex (strength 5, centred at the
+origin, freestream rho = p = 1, u = (1,1)) on the periodic square
+[-10,10]^2, 128 x 128 linear quads with vertices perturbed by up to 10% of
+the spacing (seed 0), order P = 4 (Gauss points, DG correction), gamma 1.4,
+Roe flux, RK44, global CFL 0.5.  Synthetic inputs; no dataset involved.
+
+One step = one full RK4 step (dt reduction + 4 fused stage kernels) over all
+16384 elements; DOF = nEles * nSpts * nFields = 1,638,400.  `value` is the
+mixed-precision path; the FP64 path is reported beside it.
+
+Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
+on the solver's stream; L2 is flushed (a 512 MiB write) before every step,
+outside the events.  Multi-GPU: independent replicas, one per rank
+(`scaling: weak`), time = max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, ORDER = 128, 4
+METRIC = "DOF-updates/s on 1 B200: mixed vs FP64 at stated error; adjoint/forward time"
+UNIT = "DOF-updates/s"
+WORKLOAD = "euler2d_isentropic_vortex_periodic_128x128_P4_roe_rk44_cfl0.5"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def c2_mesh():
+    from fr_learn_b200 import box2d
+
+    return box2d(NX, NX, -10.0, 10.0, -10.0, 10.0, perturb=0.1, seed=0)
+
+
+def c2_params(**kw):
+    d = dict(order=ORDER, equation=1, riemannType=1, timeType=4, dtType=1, CFL=0.5, gamma=1.4,
+             rhoBound=1.0, uBound=1.0, vBound=1.0, pBound=1.0)
+    d.update(kw)
+    return d
+
+
+def bytes_per_dof_update(nDims, P, nV, s, g):
+    """Algorithmic bytes per DOF-update (4 RK stages), the per-element model:
+    nS*nV*(2s+24) + nS*(d^2+1)*g + nF*(d+1)*g + 4*nF*nV*s + 4*nF per stage."""
+    n1 = P + 1
+    nS = n1 ** nDims
+    nF = 2 * nDims * n1 ** (nDims - 1)
+    per_stage = nS * nV * (2 * s + 24) + nS * (nDims * nDims + 1) * g + nF * (nDims + 1) * g + 4 * nF * nV * s + 4 * nF
+    return 4 * per_stage / (nS * nV)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    mesh = c2_mesh()
+    res = {}
+    solvers = {}
+    for name, prec in (("mixed", FRG_MIXED), ("fp64", FRG_FP64)):
+        s = Solver(mesh, precision=prec, **c2_params())
+        s.set_stream(stream.cuda_stream)
+        s.setInitialCondition(1)
+        solvers[name] = s
+    dof = solvers["mixed"].nEles * solvers["mixed"].nSpts * solvers["mixed"].nFields
+    clocks = None
+    for name, s in solvers.items():
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                flush.fill_(1)
+                s.update(1)
+            stream.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            launches0 = s.launch_count()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+            sampler = ClockSampler(local_rank)
+            with sampler:
+                t_wall = time.perf_counter()
+                for k in range(args.steps):
+                    flush.fill_(k & 0xFF)
+                    ev[k][0].record(stream)
+                    s.update(1)
+                    ev[k][1].record(stream)
+                stream.synchronize()
+                t_wall = time.perf_counter() - t_wall
+            torch.cuda.synchronize()
+            ms = sum(a.elapsed_time(b) for a, b in ev)
+            launches = s.launch_count() - launches0
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            torch.distributed.barrier()
+            ms = float(t.item())
+        res[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "launches": launches, "wall_s": t_wall}
+        if name == "mixed":
+            clocks = sampler.summary()
+    # accuracy of the mixed path against the FP64 path after the same steps
+    # (the FP64 path matches the FP64 oracle to 1e-12, see tests/)
+    Um, Ud = solvers["mixed"].get("U_spts"), solvers["fp64"].get("U_spts")
+    err_l2 = float(np.linalg.norm(Um - Ud) / np.linalg.norm(Ud))
+    err_linf = float(np.abs(Um - Ud).max() / np.abs(Ud).max())
+    # error of the FP64 density against the exact convected vortex
+    # (calcError, src/funcs.cpp:1902-1950, on the [-10,10]^2 period)
+    t_phys = solvers["fp64"].time
+    pos = solvers["fp64"].get("pos_spts")
+    x = np.mod(pos[..., 0] - t_phys + 10.0, 20.0) - 10.0
+    y = np.mod(pos[..., 1] - t_phys + 10.0, 20.0) - 10.0
+    g = 1.4
+    f = 1.0 - (x * x + y * y)
+    rho_ex = np.maximum((1.0 - 25.0 * (g - 1.0) / (8.0 * g * np.pi ** 2) * np.exp(f)) ** (1.0 / (g - 1.0)), 1e-10)
+    rho_err = float(np.linalg.norm(Ud[..., 0] - rho_ex) / np.linalg.norm(rho_ex))
+
+    # per-launch kernel durations (same kernels, launched without the graph)
+    stage_ms = {}
+    for name, s in solvers.items():
+        with torch.cuda.stream(stream):
+            stage_ms[name] = s.time_stages(max(3, min(50, args.steps)), flush.data_ptr(), flush.numel()).tolist()
+
+    # end to end through the C ABI with host buffers: each step uploads the
+    # state from pinned memory, runs update(), downloads the state
+    s = solvers["mixed"]
+    Uh = torch.empty((s.nSpts, s.nEles, s.nFields), dtype=torch.float64, pin_memory=True)
+    Uh.numpy()[...] = s.get("U_spts")
+    n_e2e = max(3, min(args.steps, 200))
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            s.update_host(Uh.numpy(), 1)
+        stream.synchronize()
+        e2e_ms = 0.0
+        for k in range(n_e2e):
+            flush.fill_(k & 0xFF)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s.update_host(Uh.numpy(), 1)
+            b.record(stream)
+            b.synchronize()
+            e2e_ms += a.elapsed_time(b)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    state_bytes = s.nSpts * s.nEles * s.nFields * 8
+    for sv in solvers.values():
+        sv.set_stream(None)
+    return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
+
+
+def cpu_baseline(steps=2, threads=1):
+    """The oracle (CPU restatement of the reference, which cannot run 2D
+    meshes) on the same workload, timed on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api
+
+    oracle_api.lib().orc_set_threads(threads)
+    mesh = c2_mesh()
+    p = oracle_api.params(nDims=2, **c2_params())
+    o = oracle_api.Oracle(p, mesh)
+    o.set_ic(1)
+    o.update(1)  # first iteration also recomputes the wave speeds
+    t0 = time.perf_counter()
+    o.update(steps)
+    dt = time.perf_counter() - t0
+    dof = o.nE * o.nS * o.nV
+    return dof * steps / dt, dt
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    n = max(args.gpus, world)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = max(1, min(os.cpu_count() or 1, 64))
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_api
+
+        oracle_api.lib().orc_set_threads(threads)
+        mesh = c2_mesh()
+        o = oracle_api.Oracle(oracle_api.params(nDims=2, **c2_params()), mesh)
+        o.set_ic(1)
+        dof = o.nE * o.nS * o.nV
+        # bounded sample: at most 3 warm-up steps and ~60 s of timed steps
+        for _ in range(min(args.warmup, 3)):
+            o.update(1)
+        t0 = time.perf_counter()
+        done = 0
+        while done < args.steps and (done == 0 or time.perf_counter() - t0 < 60.0):
+            o.update(1)
+            done += 1
+        secs = time.perf_counter() - t0
+        v = dof * done / secs
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": n, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * secs / done, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "nEles": o.nE, "order": ORDER, "dof": dof},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"{done} RK4 steps of the full workload (bounded to ~60 s) after "
+                                           f"{min(args.warmup, 3)} warm-up steps"},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "the reference cannot run 2D meshes (src/geo.cpp:35-37); this arm times the oracle, "
+                        "its CPU restatement, which reproduces the reference bit-for-bit on 3D cases"}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import torch
+
+        torch.distributed.init_process_group("nccl", init_method="env://",
+                                             timeout=__import__("datetime").timedelta(seconds=120))
+    dof, res, stage_ms, clocks, errs, (e2e_ms, state_bytes) = run_gpu(args, rank, world, local_rank)
+    if rank != 0:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+        return 0
+    mixed, fp64 = res["mixed"], res["fp64"]
+    value = n * dof / (mixed["ms_per_step"] * 1e-3)
+    value_fp64 = n * dof / (fp64["ms_per_step"] * 1e-3)
+    peak, peak_kind = peaks()
+    # dominant kernel: the fused RK stage kernel (mean over the 4 stages)
+    st_mixed = float(np.mean(stage_ms["mixed"][1:]))
+    st_fp64 = float(np.mean(stage_ms["fp64"][1:]))
+    b_mixed = bytes_per_dof_update(2, ORDER, 4, 4, 4) / 4 * dof  # per stage launch
+    b_fp64 = bytes_per_dof_update(2, ORDER, 4, 8, 8) / 4 * dof
+    ach = b_mixed / (st_mixed * 1e-3) / 1e9
+    ach64 = b_fp64 / (st_fp64 * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json.txt")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                traffic = json.load(f).get("mixed_dram_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+    cpu_v, cpu_s = cpu_baseline(steps=2, threads=1)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 operators/fluxes + f64 Riemann pressure & RK accumulation (mixed)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nEles": NX * NX, "order": ORDER, "dof": dof, "parallelism":
+                   f"replicas x{n}" if n > 1 else "single GPU", "l2": "flushed (512 MiB write) before every step"},
+        "fp64": {"value": value_fp64, "ms_per_step": fp64["ms_per_step"], "unit": UNIT},
+        "mixed_over_fp64": value / value_fp64,
+        "error_vs_fp64": {"rel_l2": errs[0], "rel_linf": errs[1], "steps": args.warmup + args.steps,
+                          "time": errs[3]},
+        "fp64_density_rel_l2_vs_exact_vortex": errs[2],
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "fr_stage_kernel (mixed)", "launch_ms": st_mixed,
+                     "bytes_per_launch": b_mixed,
+                     "fp64": {"achieved": ach64, "frac": ach64 / peak, "launch_ms": st_fp64,
+                              "bytes_per_launch": b_fp64},
+                     "dt_kernel_ms": stage_ms["mixed"][0]},
+        "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"2 RK4 steps of the full 128x128 P4 workload ({cpu_s:.1f} s), oracle "
+                                   "(CPU restatement; the reference cannot run 2D meshes)"},
+        "e2e": {"value": n * dof / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes,
+                "how": "frg_update_host per step: pinned host state [spt][ele][field] -> device, one RK4 step, "
+                       "state -> host"},
+        "gpu_launches": mixed["launches"],
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -235,7 +235,7 @@ struct frg_solver {
   int nV = 0, nS = 0, nF = 0, nE = 0, nBlk = 0, nRK = 0;
   size_t sstore = 8;  // bytes of the stored type
   std::vector<double> RKa, RKb;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr, ownStream = nullptr;
   // device buffers
   double *U = nullptr, *U0 = nullptr, *Acc = nullptr, *divF[5] = {nullptr};
   void *W[2] = {nullptr, nullptr}, *tr[2] = {nullptr, nullptr};
@@ -395,13 +395,17 @@ frg_status launch_wavesp(frg_solver *s) {
   return post_launch(s);
 }
 
-// One fused step (the body of solver::update) on the stream.
-frg_status enqueue_step(frg_solver *s, bool firstIter) {
+// One fused step (the body of solver::update) on the stream.  With `ev`
+// (2 + nRK events) an event is recorded before the dt kernels and after each
+// launch, for frg_time_stages.
+frg_status enqueue_step(frg_solver *s, bool firstIter, cudaEvent_t *ev = nullptr) {
   frg_status st;
+  if (ev) CK(cudaEventRecord(ev[0], s->stream));
   if (s->p.dtType != 0) {
     if (firstIter && (st = launch_wavesp(s))) return st;
     if ((st = launch_dt(s))) return st;
   }
+  if (ev) CK(cudaEventRecord(ev[1], s->stream));
   const int nRK = s->nRK;
   const bool jam = s->p.timeType == 5;
   for (int k = 0; k < nRK; k++) {
@@ -423,6 +427,7 @@ frg_status enqueue_step(frg_solver *s, bool firstIter) {
       a.divF = s->divF[0];
     }
     if ((st = launch_stage_args(s, a))) return st;
+    if (ev) CK(cudaEventRecord(ev[2 + k], s->stream));
     s->curTr ^= 1;
   }
   return FRG_OK;
@@ -570,7 +575,8 @@ frg_status frg_destroy(frg_solver *s) {
   for (double *q : dp) if (q) cudaFree(q);
   void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->nbr, s->err, s->ticket};
   for (void *q : vp) if (q) cudaFree(q);
-  if (s->stream) cudaStreamDestroy(s->stream);
+  cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy
+  if (own) cudaStreamDestroy(own);
   delete s;
   return FRG_OK;
 }
@@ -850,6 +856,42 @@ frg_status frg_sync(frg_solver *s) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
   CK(cudaStreamSynchronize(s->stream));
   return FRG_OK;
+}
+
+frg_status frg_set_stream(frg_solver *s, void *stream) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  CK(cudaStreamSynchronize(s->stream));
+  if (!s->ownStream) s->ownStream = s->stream;
+  s->stream = stream ? (cudaStream_t)stream : s->ownStream;
+  return FRG_OK;
+}
+
+frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long long flushBytes, double *ms_out) {
+  if (!s || !ms_out || nsteps < 1) return fail(FRG_ERR_ARG, "bad arguments");
+  if (s->p.timeType == 0 && s->p.dtType != 0) return fail(FRG_ERR_ARG, "Forward Euler with CFL dt is not fused");
+  frg_status st;
+  if ((st = ensure_traces(s))) return st;
+  const int nEv = 2 + s->nRK;
+  std::vector<cudaEvent_t> ev(nEv);
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(1 + s->nRK, 0.0);
+  for (int n = 0; n < nsteps && !st; n++) {
+    if (flush) CK(cudaMemsetAsync(flush, n & 0xff, flushBytes, s->stream));
+    s->iter++;
+    const bool fi = s->p.dtType != 0 && s->iter == s->initIter + 1;
+    st = enqueue_step(s, fi, ev.data());
+    if (st) break;
+    CK(cudaEventSynchronize(ev[nEv - 1]));
+    for (int k = 0; k <= s->nRK; k++) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      acc[k] += ms;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (st) return st;
+  for (int k = 0; k <= s->nRK; k++) ms_out[k] = acc[k] / nsteps;
+  return check_flags(s);
 }
 
 frg_status frg_launch_count(const frg_solver *s, long long *count) {

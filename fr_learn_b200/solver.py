@@ -96,6 +96,8 @@ def lib():
         "frg_get_time": ([vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)], i),
         "frg_set_iter": ([vp, i, i], i), "frg_sync": ([vp], i),
         "frg_launch_count": ([vp, C.POINTER(C.c_longlong)], i),
+        "frg_set_stream": ([vp, vp], i),
+        "frg_time_stages": ([vp, i, vp, C.c_ulonglong, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -237,6 +239,18 @@ class Solver:
         n = C.c_longlong()
         _check(lib().frg_launch_count(self.h, C.byref(n)))
         return n.value
+
+    def set_stream(self, stream_ptr):
+        """Run on a caller's cudaStream_t (an int handle, e.g. torch's
+        ``stream.cuda_stream``); None restores the solver's own stream."""
+        _check(lib().frg_set_stream(self.h, stream_ptr))
+
+    def time_stages(self, nsteps, flush_ptr=None, flush_bytes=0):
+        """Mean per-launch device time (ms) of [dt kernels, stage 0..nRK-1]."""
+        nrk = {0: 1, 2: 2, 4: 4, 5: 4}[self.params["timeType"]]
+        out = np.zeros(1 + nrk)
+        _check(lib().frg_time_stages(self.h, nsteps, flush_ptr, flush_bytes, out.ctypes.data))
+        return out
 
 
 def inspect_geometry(mesh: Mesh, which: str, **params) -> np.ndarray:

@@ -163,6 +163,15 @@ frg_status frg_get_time(const frg_solver *s, double *time, double *dt, int *iter
 frg_status frg_set_iter(frg_solver *s, int iter, int initIter);
 /* Synchronise the handle's stream (all work finished). */
 frg_status frg_sync(frg_solver *s);
+/* Run subsequent work on `stream` (a cudaStream_t; NULL restores the
+ * handle's own stream).  Pending work on the previous stream is finished first. */
+frg_status frg_set_stream(frg_solver *s, void *stream);
+/* Measurement hook: nsteps fused steps launched one kernel at a time (no
+ * graph) with CUDA events around every launch.  If flush != NULL, flushBytes
+ * of it are overwritten before each step (evicts L2).  ms_out[0] = mean time
+ * of the per-step dt / wave-speed kernels, ms_out[1 + k] = mean time of RK
+ * stage k's kernel, all in milliseconds ([1 + nRK] entries). */
+frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long long flushBytes, double *ms_out);
 /* Device-side launch counter: kernels launched by this handle so far. */
 frg_status frg_launch_count(const frg_solver *s, long long *count);
 
