@@ -24,9 +24,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC"] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
-CU_SOURCES = ["frgpu.cu"]
+CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu"]
 CXX_SOURCES = ["setup.cpp"]
-HEADERS = ["kernels.cuh", "physics.cuh", "setup.h"]
+HEADERS = ["kernels.cuh", "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
 
 
 def _nvcc():
@@ -67,14 +67,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if force or _newer(o, [s] + hdrs):
             _run([_cxx()] + CXX_FLAGS + ["-c", s, "-o", o])
         objs.append(o)
+    jobs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or _newer(o, [s] + hdrs):
-            r = _run([_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o])
+            jobs.append([_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o])
+        objs.append(o)
+    # the kernel units are independent: compile them in parallel
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in ex.map(_run, jobs):
             if verbose:
                 sys.stderr.write(r.stderr)
-        objs.append(o)
     if force or _newer(LIB, objs):
         _run([_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
     return LIB

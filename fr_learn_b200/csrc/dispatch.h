@@ -1,0 +1,41 @@
+// dispatch.h -- host-side table of the kernels compiled for one configuration
+// (dimension, order, fields, precision, boundary faces, Riemann solver).
+// The instantiations live in four translation units (stage_{2d,3d}_{f64,f32}.cu)
+// compiled in parallel; each also owns a copy of the 1D operator tables.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "physics.cuh"
+#include "setup.h"
+
+namespace frg {
+
+struct KernelSet {
+  void (*stage)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
+  void (*trace)(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) = nullptr;
+  void (*wavesp)(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph,
+                 cudaStream_t st) = nullptr;
+  int TE = 0;       // elements per block
+  int NT = 0;       // threads per block
+  size_t smem = 0;  // dynamic shared memory per block
+};
+
+struct KernelKey {
+  int nDims, P, NV, precision, bc, riemann;
+};
+
+// Fills `k` for the key, or returns false with `err` set.
+bool select_2d_f64(const KernelKey &key, KernelSet &k, std::string &err);
+bool select_2d_f32(const KernelKey &key, KernelSet &k, std::string &err);
+bool select_3d_f64(const KernelKey &key, KernelSet &k, std::string &err);
+bool select_3d_f32(const KernelKey &key, KernelSet &k, std::string &err);
+
+// Uploads the 1D operator tables (all schemes, orders 0..5) into each unit.
+cudaError_t upload_tables_2d_f64();
+cudaError_t upload_tables_2d_f32();
+cudaError_t upload_tables_3d_f64();
+cudaError_t upload_tables_3d_f32();
+
+}  // namespace frg

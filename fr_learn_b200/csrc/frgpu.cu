@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/frgpu.h"
+#include "dispatch.h"
 #include "kernels.cuh"
 #include "setup.h"
 
@@ -150,75 +151,10 @@ __global__ void fr_cast_kernel(const double *in, S *out, long n) {
   if (i < n) out[i] = (S)in[i];
 }
 
-// ------------------------------------------------------------ dispatch table
-struct KernelSet {
-  void (*stage)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
-  void (*trace)(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) = nullptr;
-  void (*wavesp)(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph,
-                 cudaStream_t st) = nullptr;
-  int TE = 0;
-  size_t smem = 0;
-};
-
-template <class C, typename R, typename S>
-void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
-  fr_stage_kernel<C, R, S><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
-}
-template <class C, typename R, typename S>
-void launch_trace(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) {
-  long n = (long)C::NF * nE;
-  fr_trace_kernel<C, R, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U, static_cast<S *>(tr), nE, vcjh);
-}
-template <int DIM, int NV, typename S>
-void launch_wavesp(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph, cudaStream_t st) {
-  long n = (long)NF * nE;
-  fr_wavesp_kernel<DIM, NV, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<const S *>(tr), nrmOwn, ws,
-                                                                             NF, nE, ph);
-}
-
-template <int DIM, int P, int NV, typename R, typename S>
-bool make_set(KernelSet &k, std::string &err) {
-  using C = Cfg<DIM, P, NV>;
-  using T = Tile<C, R>;
-  k.stage = &launch_stage<C, R, S>;
-  k.trace = &launch_trace<C, R, S>;
-  k.wavesp = &launch_wavesp<DIM, NV, S>;
-  k.TE = T::TE;
-  k.smem = T::SMEM;
-  cudaError_t e = cudaFuncSetAttribute(fr_stage_kernel<C, R, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)T::SMEM);
-  if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
-  return true;
-}
-
-template <int DIM, int NV, typename R, typename S>
-bool select_order(int P, KernelSet &k, std::string &err) {
-  switch (P) {
-    case 1: return make_set<DIM, 1, NV, R, S>(k, err);
-    case 2: return make_set<DIM, 2, NV, R, S>(k, err);
-    case 3: return make_set<DIM, 3, NV, R, S>(k, err);
-    case 4: return make_set<DIM, 4, NV, R, S>(k, err);
-    case 5:
-      if constexpr (DIM == 2) return make_set<DIM, 5, NV, R, S>(k, err);
-      break;
-  }
-  err = "order not available for this dimension (2D: 1..5, 3D: 1..4)";
-  return false;
-}
-
-bool select_kernels(int nDims, int P, int NV, int prec, KernelSet &k, std::string &err) {
-  if (prec == FRG_FP64) {
-    if (nDims == 2 && NV == 1) return select_order<2, 1, double, double>(P, k, err);
-    if (nDims == 2 && NV == 4) return select_order<2, 4, double, double>(P, k, err);
-    if (nDims == 3 && NV == 1) return select_order<3, 1, double, double>(P, k, err);
-    if (nDims == 3 && NV == 5) return select_order<3, 5, double, double>(P, k, err);
-  } else {
-    if (nDims == 2 && NV == 1) return select_order<2, 1, float, float>(P, k, err);
-    if (nDims == 2 && NV == 4) return select_order<2, 4, float, float>(P, k, err);
-    if (nDims == 3 && NV == 1) return select_order<3, 1, float, float>(P, k, err);
-    if (nDims == 3 && NV == 5) return select_order<3, 5, float, float>(P, k, err);
-  }
-  err = "unsupported dimension / field count";
+bool select_kernels(const KernelKey &key, KernelSet &k, std::string &err) {
+  if (key.nDims == 2) return key.precision == FRG_FP64 ? select_2d_f64(key, k, err) : select_2d_f32(key, k, err);
+  if (key.nDims == 3) return key.precision == FRG_FP64 ? select_3d_f64(key, k, err) : select_3d_f32(key, k, err);
+  err = "unsupported dimension";
   return false;
 }
 
@@ -254,7 +190,6 @@ struct frg_solver {
 
 namespace {
 thread_local std::string g_err;
-bool g_tables = false;
 
 frg_status fail(frg_status st, const char *fmt, ...) {
   char buf[512];
@@ -272,28 +207,15 @@ frg_status fail(frg_status st, const char *fmt, ...) {
                                        __FILE__, __LINE__);                                      \
   } while (0)
 
-frg_status upload_tables() {
-  if (g_tables) return FRG_OK;
-  static OpTab<double> hd[4][KMAXP + 1];
-  static OpTab<float> hf[4][KMAXP + 1];
-  for (int sch = 0; sch < 4; sch++)
-    for (int P = 0; P <= KMAXP; P++) {
-      if (sch == 3 && P < 2) continue;  // C+ is tabulated for P = 2..5 only
-      if (sch == 2 && P == 0) continue;
-      Ops1D o = build_ops1d(P, sch);
-      OpTab<double> &d = hd[sch][P];
-      OpTab<float> &f = hf[sch][P];
-      for (int i = 0; i <= KMAXP; i++) {
-        d.lag[0][i] = o.lag[0][i]; d.lag[1][i] = o.lag[1][i];
-        d.gL[i] = o.gL[i]; d.gR[i] = o.gR[i]; d.w[i] = o.w[i];
-        f.lag[0][i] = (float)o.lag[0][i]; f.lag[1][i] = (float)o.lag[1][i];
-        f.gL[i] = (float)o.gL[i]; f.gR[i] = (float)o.gR[i]; f.w[i] = (float)o.w[i];
-        for (int j = 0; j <= KMAXP; j++) { d.dlag[i][j] = o.dlag[i][j]; f.dlag[i][j] = (float)o.dlag[i][j]; }
-      }
-    }
-  CK(cudaMemcpyToSymbol(c_opd, hd, sizeof hd));
-  CK(cudaMemcpyToSymbol(c_opf, hf, sizeof hf));
-  g_tables = true;
+// Each kernel unit holds its own copy of the 1D operator tables.
+bool g_tables[2][2] = {{false, false}, {false, false}};
+frg_status upload_tables(int nDims, int prec) {
+  bool &done = g_tables[nDims - 2][prec != FRG_FP64];
+  if (done) return FRG_OK;
+  cudaError_t e = nDims == 2 ? (prec == FRG_FP64 ? upload_tables_2d_f64() : upload_tables_2d_f32())
+                             : (prec == FRG_FP64 ? upload_tables_3d_f64() : upload_tables_3d_f32());
+  if (e != cudaSuccess) return fail(FRG_ERR_CUDA, "operator tables: %s", cudaGetErrorString(e));
+  done = true;
   return FRG_OK;
 }
 
@@ -487,8 +409,9 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   if (st) return fail(st, "%s", err.c_str());
   s->ops = build_ops1d(p.order, p.vcjhScheme);
   s->nS = s->g.nS; s->nF = s->g.nF; s->nE = s->g.nE;
-  if ((st = upload_tables())) return st;
-  if (!select_kernels(p.nDims, p.order, s->nV, p.precision, s->ks, err)) return fail(FRG_ERR_ARG, "%s", err.c_str());
+  if ((st = upload_tables(p.nDims, p.precision))) return st;
+  KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType};
+  if (!select_kernels(key, s->ks, err)) return fail(FRG_ERR_ARG, "%s", err.c_str());
   s->sstore = p.precision == FRG_FP64 ? 8 : 4;
   s->nBlk = (s->nE + s->ks.TE - 1) / s->ks.TE;
   CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));

@@ -44,9 +44,10 @@ struct OpTab {
   R gL[KMAXP + 1], gR[KMAXP + 1];
   R w[KMAXP + 1];
 };
-// Defined here: the library is one CUDA translation unit (frgpu.cu).
-__constant__ OpTab<double> c_opd[4][KMAXP + 1];
-__constant__ OpTab<float> c_opf[4][KMAXP + 1];
+// Each CUDA translation unit that includes this header holds its own copy of
+// the tables (internal linkage) and uploads it through its own entry point.
+static __constant__ OpTab<double> c_opd[4][KMAXP + 1];
+static __constant__ OpTab<float> c_opf[4][KMAXP + 1];
 
 template <typename R>
 __device__ __forceinline__ const OpTab<R> &optab(int vcjh, int P);
@@ -169,9 +170,12 @@ struct StageArgs {
 // ----------------------------------------------------------------------------
 // The fused stage kernel (inviscid Euler or scalar advection).
 // R: arithmetic type; S: stored type of stage states, traces and metrics.
+// BC: the mesh has boundary faces (else the ghost-state code is not built);
+// RS: interior Riemann solver, 0 Rusanov, 1 Roe (boundaries always Rusanov,
+// src/face.cpp:142-145).  Two resident blocks per SM cap registers at 128.
 // ----------------------------------------------------------------------------
-template <class C, typename R, typename S>
-__global__ void __launch_bounds__(C::NT, 1) fr_stage_kernel(const StageArgs a) {
+template <class C, typename R, typename S, bool BC, int RS>
+__global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
   using T = Tile<C, R>;
   constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -254,8 +258,11 @@ __global__ void __launch_bounds__(C::NT, 1) fr_stage_kernel(const StageArgs a) {
       for (int v = 0; v < NV; v++) oth[v] = (R)trIn[(size_t)v * NF * nE + t];
     } else {
       bc = -1 - code;
-      if constexpr (NV == 1) {
-        oth[0] = 0;  // advection boundaries keep a zero ghost state (src/boundFace.cpp:274)
+      if constexpr (NV == 1 || !BC) {
+        // advection boundaries keep a zero ghost state (src/boundFace.cpp:274)
+#pragma unroll
+        for (int v = 0; v < NV; v++) oth[v] = 0;
+        if constexpr (!BC) atomicOr(a.err, ERRF_BC);
       } else {
         double ul[NV], ur[NV], nd[DIM];
 #pragma unroll
@@ -273,9 +280,13 @@ __global__ void __launch_bounds__(C::NT, 1) fr_stage_kernel(const StageArgs a) {
     R ws = -1;
     if constexpr (NV == 1) {
       ws = lax_friedrichs<DIM, R>(UL[0], UR[0], n, Fn, ph);
+    } else if constexpr (RS == 0 || DIM == 3) {
+      ws = rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
+    } else if constexpr (BC) {
+      if (code < 0) ws = rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
+      else roe2d<R, double>(UL, UR, n, Fn, ph);
     } else {
-      if (code < 0 || ph.riemann == 0 || DIM == 3) ws = rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
-      else if constexpr (DIM == 2) roe2d<R, double>(UL, UR, n, Fn, ph);
+      roe2d<R, double>(UL, UR, n, Fn, ph);
     }
     if ((a.flags & SF_WAVESP) && !right && ws >= 0) a.waveSp[(size_t)f * nE + eg] = (double)ws;
 #pragma unroll
@@ -414,30 +425,5 @@ __global__ void fr_wavesp_kernel(const S *__restrict__ tr, const double *__restr
   }
   waveSp[(size_t)f * nE + e] = ws;
 }
-
-// ele::calcDt (src/ele.cpp:1086-1105) per element, then the global minimum:
-// warp-shuffle min inside a block, per-block minima, and the last block to
-// finish reduces those (threadfence + ticket counter).
-__global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__restrict__ dA,
-                             const double *__restrict__ vol, const double *__restrict__ wsurf, int NF, int NFF,
-                             int nE, double cflFac, double *eleDt, double *blockMin, unsigned *ticket,
-                             double *dtOut, unsigned *err);
-
-// U = U0 - rkval * divF / detJ * dt (timeStepA) or U -= rkb * divF / detJ * dt
-// (timeStepB), [NV][NS][nE].
-__global__ void fr_timestep_kernel(double *U, const double *U0, const double *divF, const double *detJ,
-                                   const double *dt, int dtLocal, double coef, int modeB, int NS, int nE,
-                                   long total);
-
-// Residual norms of ele::getNormResidual (src/ele.cpp:1882-1903): per-block
-// partial sums over elements in a fixed order, then the last block adds them.
-__global__ void fr_norm_kernel(const double *divF, const double *detJ, const double *wvol, int NV, int NS, int nE,
-                               int normType, double *partial, unsigned *ticket, double *out);
-
-// Layout conversions [pt][e][v] (reference) <-> [v][pt][e] (device).
-__global__ void fr_to_device_layout(const double *ref, double *dev, int NV, int NPT, int nE);
-__global__ void fr_to_ref_layout(const double *dev, double *ref, int NV, int NPT, int nE);
-template <typename S>
-__global__ void fr_cast_kernel(const double *in, S *out, long n);
 
 }  // namespace frg

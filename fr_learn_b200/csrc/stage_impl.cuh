@@ -1,0 +1,111 @@
+// stage_impl.cuh -- launchers and the instantiation switch shared by the
+// per-configuration translation units.  Include once per unit after defining
+// FRG_UNIT_DIM (2 or 3), FRG_UNIT_R / FRG_UNIT_S (arithmetic / stored type)
+// and FRG_UNIT_NAME (suffix of the exported functions).
+#pragma once
+#include "dispatch.h"
+#include "kernels.cuh"
+
+namespace frg {
+namespace {
+
+template <class C, typename R, typename S, bool BC, int RS>
+void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
+  fr_stage_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
+}
+template <class C, typename R, typename S>
+void launch_trace(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) {
+  long n = (long)C::NF * nE;
+  fr_trace_kernel<C, R, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U, static_cast<S *>(tr), nE, vcjh);
+}
+template <int DIM, int NV, typename S>
+void launch_wavesp(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph, cudaStream_t st) {
+  long n = (long)NF * nE;
+  fr_wavesp_kernel<DIM, NV, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<const S *>(tr), nrmOwn, ws,
+                                                                             NF, nE, ph);
+}
+
+template <class C, typename R, typename S, bool BC, int RS>
+bool make_set(KernelSet &k, std::string &err) {
+  using T = Tile<C, R>;
+  k.stage = &launch_stage<C, R, S, BC, RS>;
+  k.trace = &launch_trace<C, R, S>;
+  k.wavesp = &launch_wavesp<C::DIM, C::NV, S>;
+  k.TE = T::TE;
+  k.NT = C::NT;
+  k.smem = T::SMEM;
+  auto fn = fr_stage_kernel<C, R, S, BC, RS>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+template <int DIM, int P, int NV, typename R, typename S>
+bool make_variant(const KernelKey &key, KernelSet &k, std::string &err) {
+  using C = Cfg<DIM, P, NV>;
+  if constexpr (NV == 1 || DIM == 3) {
+    return key.bc ? make_set<C, R, S, true, 0>(k, err) : make_set<C, R, S, false, 0>(k, err);
+  } else {
+    if (key.riemann == 1)
+      return key.bc ? make_set<C, R, S, true, 1>(k, err) : make_set<C, R, S, false, 1>(k, err);
+    return key.bc ? make_set<C, R, S, true, 0>(k, err) : make_set<C, R, S, false, 0>(k, err);
+  }
+}
+
+template <int DIM, int NV, typename R, typename S>
+bool select_order(const KernelKey &key, KernelSet &k, std::string &err) {
+  switch (key.P) {
+    case 1: return make_variant<DIM, 1, NV, R, S>(key, k, err);
+    case 2: return make_variant<DIM, 2, NV, R, S>(key, k, err);
+    case 3: return make_variant<DIM, 3, NV, R, S>(key, k, err);
+    case 4: return make_variant<DIM, 4, NV, R, S>(key, k, err);
+    case 5:
+      if constexpr (DIM == 2) return make_variant<DIM, 5, NV, R, S>(key, k, err);
+      break;
+  }
+  err = "order not available for this dimension (2D: 1..5, 3D: 1..4)";
+  return false;
+}
+
+template <typename R, typename S>
+cudaError_t upload_tables_impl() {
+  static OpTab<double> hd[4][KMAXP + 1];
+  static OpTab<float> hf[4][KMAXP + 1];
+  for (int sch = 0; sch < 4; sch++)
+    for (int P = 0; P <= KMAXP; P++) {
+      if ((sch == 3 && P < 2) || (sch == 2 && P == 0)) continue;  // eta undefined there
+      Ops1D o = build_ops1d(P, sch);
+      OpTab<double> &d = hd[sch][P];
+      OpTab<float> &f = hf[sch][P];
+      for (int i = 0; i <= KMAXP; i++) {
+        d.lag[0][i] = o.lag[0][i]; d.lag[1][i] = o.lag[1][i];
+        d.gL[i] = o.gL[i]; d.gR[i] = o.gR[i]; d.w[i] = o.w[i];
+        f.lag[0][i] = (float)o.lag[0][i]; f.lag[1][i] = (float)o.lag[1][i];
+        f.gL[i] = (float)o.gL[i]; f.gR[i] = (float)o.gR[i]; f.w[i] = (float)o.w[i];
+        for (int j = 0; j <= KMAXP; j++) { d.dlag[i][j] = o.dlag[i][j]; f.dlag[i][j] = (float)o.dlag[i][j]; }
+      }
+    }
+  cudaError_t e = cudaMemcpyToSymbol(c_opd, hd, sizeof hd);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_opf, hf, sizeof hf);
+  return e;
+}
+
+}  // namespace
+}  // namespace frg
+
+#define FRG_CAT2(a, b) a##b
+#define FRG_CAT(a, b) FRG_CAT2(a, b)
+
+namespace frg {
+bool FRG_CAT(select_, FRG_UNIT_NAME)(const KernelKey &key, KernelSet &k, std::string &err) {
+  using R = FRG_UNIT_R;
+  using S = FRG_UNIT_S;
+  if (key.NV == 1) return select_order<FRG_UNIT_DIM, 1, R, S>(key, k, err);
+  if (key.NV == FRG_UNIT_DIM + 2) return select_order<FRG_UNIT_DIM, FRG_UNIT_DIM + 2, R, S>(key, k, err);
+  err = "unsupported field count";
+  return false;
+}
+cudaError_t FRG_CAT(upload_tables_, FRG_UNIT_NAME)() { return upload_tables_impl<FRG_UNIT_R, FRG_UNIT_S>(); }
+}  // namespace frg
