@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -615,6 +616,62 @@ frg_status frg_set_initial_condition(frg_solver *s, int icType, double a0) {
   frg_status st = initial_condition(s->p, s->g, icType, a0, U, err);
   if (st) return fail(st, "%s", err.c_str());
   return frg_upload(s, FRG_U_SPTS, U.data());
+}
+
+}  // extern "C"
+
+// ---- scratch of frg_calc_residual_noalloc
+// The flux-point traces of the allocation-free residual live in this fixed
+// array (16 MiB, 256-byte aligned), so that entry point calls no allocator.
+// It is part of the library's device image: every GPU that loads the library
+// holds it until the process exits.  Host code must not use the symbol as a
+// pointer (it is a host-side stand-in); the device address is looked up once
+// per device with cudaGetSymbolAddress and passed to the kernels.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+namespace {
+constexpr int kMaxDevices = 64;
+void *g_noalloc_addr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" {
+
+frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double *divF_dev, void *stream) {
+  if (!s || !U_dev || !divF_dev) return fail(FRG_ERR_ARG, "null argument");
+  const size_t need = (size_t)s->nV * s->nF * s->nE * s->sstore;
+  if (need > kNoAllocScratchBytes)
+    return fail(FRG_ERR_ARG, "frg_calc_residual_noalloc: traces need %zu bytes, the scratch array holds %zu", need,
+                kNoAllocScratchBytes);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(FRG_ERR_ARG, "device index %d out of range", dev);
+  void *scratch = nullptr;
+  {
+    // set-up once per device, with that device current
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void *p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return fail(FRG_ERR_CUDA, "cudaGetSymbolAddress(noalloc scratch): %s", cudaGetErrorString(e));
+      g_noalloc_addr[dev] = p;
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+  // traces of the caller's state into the scratch array, then the residual
+  s->ks.trace(U_dev, scratch, s->nE, s->p.vcjhScheme, st);
+  CK(cudaGetLastError());
+  StageArgs a = base_args(s);
+  a.Uin_d = U_dev;
+  a.trIn = scratch;
+  a.divF = divF_dev;
+  a.flags = SF_RESIDUAL;
+  s->ks.stage(&a, s->nBlk, s->ks.smem, st);
+  CK(cudaGetLastError());
+  s->launches += 2;
+  return FRG_OK;
 }
 
 frg_status frg_calc_residual(frg_solver *s, int step) {

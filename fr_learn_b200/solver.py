@@ -97,6 +97,7 @@ def lib():
         "frg_set_iter": ([vp, i, i], i), "frg_sync": ([vp], i),
         "frg_launch_count": ([vp, C.POINTER(C.c_longlong)], i),
         "frg_set_stream": ([vp, vp], i),
+        "frg_calc_residual_noalloc": ([vp, vp, vp, vp], i),
         "frg_time_stages": ([vp, i, vp, C.c_ulonglong, vp], i),
     }
     for name, (args, res) in sig.items():
@@ -178,6 +179,14 @@ class Solver:
 
     def calcResidual(self, step=0):
         _check(lib().frg_calc_residual(self.h, step))
+
+    def calcResidual_noalloc(self, U_dev_ptr, divF_dev_ptr, stream_ptr=None):
+        """Residual of a caller-owned device state into a caller-owned device
+        array ([nFields][nSpts][nEles]), with no device allocation: for callers
+        whose device memory is all pre-planned or owned by another manager.
+        Traces go to the library's fixed 16 MiB scratch array (see
+        include/frgpu.h); overlapping calls race on it."""
+        _check(lib().frg_calc_residual_noalloc(self.h, U_dev_ptr, divF_dev_ptr, stream_ptr))
 
     def timeStepA(self, step, RKval):
         _check(lib().frg_time_step_a(self.h, step, RKval))

@@ -146,6 +146,31 @@ frg_status frg_copy_u0_to_u(frg_solver *s);
  * (ele::calcWaveSpFpts), then dt = min over elements (warp-shuffle reduction). */
 frg_status frg_calc_dt(frg_solver *s, double *dt_out);
 
+/* Allocation-free residual.  This entry point has no counterpart in the
+ * reference.  It is for callers that must not allocate device memory when
+ * they evaluate a residual: code running under a memory manager that owns
+ * every device allocation, a real-time loop where cudaMalloc's implicit
+ * synchronisation is not allowed, or a host application that pre-plans its
+ * whole memory footprint.  It computes divF_spts (solver::calcResidual's
+ * result, without touching the handle's wave speeds) of the caller's state
+ * `U_dev` into the caller's `divF_dev`, both device arrays laid out
+ * [nFields][nSpts][nEles] (element index fastest), on `stream` (NULL: the
+ * handle's stream).  The handle only supplies the geometry and operators
+ * built by frg_create.
+ *
+ * The flux-point traces it needs go to a fixed scratch array of 16 MiB in
+ * device memory that the library declares statically: every GPU that loads
+ * the library keeps it until the process exits.  Meshes whose traces
+ * (nFields * nFpts * nEles values, 8 bytes each in FP64 mode, 4 in mixed
+ * mode) exceed 16 MiB are rejected with FRG_ERR_ARG.  The first call on a
+ * device looks up the scratch array's device address (no allocation); make
+ * that first call before any stream capture.  All calls share the one scratch
+ * array and it keeps the last call's contents; every value a call reads is
+ * written by the same call first, so nothing needs clearing.  Calls that
+ * overlap on the GPU (different streams, or several handles at once) race on
+ * the scratch array: serialise them. */
+frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double *divF_dev, void *stream);
+
 /* nsteps iterations of the reference main loop body (iter++; update()), as
  * one fused kernel per RK stage replayed from a CUDA graph.  Device-resident:
  * no host transfer.  Checks the NaN / dt flags after the last step. */
