@@ -62,6 +62,25 @@ def bytes_per_dof_update(nDims, P, nV, s, g):
     return 4 * per_stage / (nS * nV)
 
 
+def max_over_ranks(x, world, device=None):
+    """Maximum of a per-rank time over all ranks (every rank calls this in
+    the same order); a no-op on one rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def throughput(n_ranks, dof, ms_per_step):
+    """Whole-job DOF-updates/s: every rank advances `dof` unknowns per step
+    (replicas), the job takes the slowest rank's time."""
+    return n_ranks * dof / (ms_per_step * 1e-3)
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -164,12 +183,8 @@ def run_gpu(args, rank, world, local_rank):
             torch.cuda.synchronize()
             ms = sum(a.elapsed_time(b) for a, b in ev)
             launches = s.launch_count() - launches0
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            torch.distributed.barrier()
-            ms = float(t.item())
-        res[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "launches": launches, "wall_s": t_wall}
+        ms = max_over_ranks(ms, world, dev)
+        res[name] ={"ms_total": ms, "ms_per_step": ms / args.steps, "launches": launches, "wall_s": t_wall}
         if name == "mixed":
             clocks = sampler.summary()
     # accuracy of the mixed path against the FP64 path after the same steps
@@ -213,10 +228,7 @@ def run_gpu(args, rank, world, local_rank):
             b.record(stream)
             b.synchronize()
             e2e_ms += a.elapsed_time(b)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, dev)
     state_bytes = s.nSpts * s.nEles * s.nFields * 8
     for sv in solvers.values():
         sv.set_stream(None)
@@ -303,8 +315,8 @@ def main():
             torch.distributed.destroy_process_group()
         return 0
     mixed, fp64 = res["mixed"], res["fp64"]
-    value = n * dof / (mixed["ms_per_step"] * 1e-3)
-    value_fp64 = n * dof / (fp64["ms_per_step"] * 1e-3)
+    value = throughput(n, dof, mixed["ms_per_step"])
+    value_fp64 = throughput(n, dof, fp64["ms_per_step"])
     peak, peak_kind = peaks()
     # dominant kernel: the fused RK stage kernel (mean over the 4 stages)
     st_mixed = float(np.mean(stage_ms["mixed"][1:]))
@@ -344,7 +356,7 @@ def main():
         "cpu_baseline": {"value": cpu_v, "unit": UNIT, "cores": 1, "kind": "port",
                          "sample": f"2 RK4 steps of the full 128x128 P4 workload ({cpu_s:.1f} s), oracle "
                                    "(CPU restatement; the reference cannot run 2D meshes)"},
-        "e2e": {"value": n * dof / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+        "e2e": {"value": throughput(n, dof, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes,
                 "how": "frg_update_host per step: pinned host state [spt][ele][field] -> device, one RK4 step, "
                        "state -> host"},

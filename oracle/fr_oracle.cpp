@@ -1046,6 +1046,40 @@ extern "C" {
 
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 
+void orc_point_flux(const orc_params *p, const double *U, const double *gradU, double *Finv, double *Fvis) {
+  int d = p->nDims, nV = p->equation == 0 ? 1 : d + 2;
+  double F[3][5] = {{0}}, G[3][5] = {{0}};
+  inviscidFlux(*p, U, F);
+  if (gradU && Fvis) {
+    if (p->equation == 1) viscousFlux(*p, U, gradU, G);
+    else viscousFluxAD(*p, gradU, G);
+  }
+  for (int a = 0; a < d; a++)
+    for (int k = 0; k < nV; k++) {
+      Finv[a * nV + k] = F[a][k];
+      if (Fvis) Fvis[a * nV + k] = G[a][k];
+    }
+}
+double orc_point_rusanov(const orc_params *p, const double *UL, const double *UR, const double *n, double *Fn) {
+  return rusanov(*p, UL, UR, n, Fn);
+}
+void orc_point_roe(const orc_params *p, const double *UL, const double *UR, const double *n, double *Fn) {
+  roe(*p, UL, UR, n, Fn);
+}
+double orc_point_lf(const orc_params *p, double uL, double uR, const double *n, double *Fn) {
+  return laxFriedrichs(*p, uL, uR, n, Fn);
+}
+void orc_point_ldg_uc(const orc_params *p, const double *UL, const double *UR, const double *n, double *UC) {
+  int d = p->nDims, nV = d + 2;
+  double pf = p->penFact;
+  if (d == 2) { if (n[0] + n[1] < 0) pf = -p->penFact; }
+  else if (n[0] + n[1] + sqrt(2.) * n[2] < 0) pf = -p->penFact;
+  for (int k = 0; k < nV; k++) UC[k] = 0.5 * (UL[k] + UR[k]) - pf * (UL[k] - UR[k]);
+}
+void orc_point_bc(const orc_params *p, int bcType, const double *UL, const double *n, double *UR) {
+  applyBC(*p, bcType, UL, n, UR);
+}
+
 orc_solver *orc_create(const orc_params *p, int nEles, int nNodes, const double *xv, const int *c2v, const int *bc) {
   orc_solver *s = new orc_solver();
   s->p = *p;

@@ -89,6 +89,15 @@ int orc_get_iter(const orc_solver *s);
 void orc_residual_norm(const orc_solver *s, int normType, double *out);
 void orc_set_threads(int n);
 
+/* Pointwise routines, exposed for known-answer tests against the reference.
+ * Fluxes are [nDims][nFields]; gradU is [nDims][nFields]. */
+void orc_point_flux(const orc_params *p, const double *U, const double *gradU, double *Finv, double *Fvis);
+double orc_point_rusanov(const orc_params *p, const double *UL, const double *UR, const double *n, double *Fn);
+void orc_point_roe(const orc_params *p, const double *UL, const double *UR, const double *n, double *Fn);
+double orc_point_lf(const orc_params *p, double uL, double uR, const double *n, double *Fn);
+void orc_point_ldg_uc(const orc_params *p, const double *UL, const double *UR, const double *n, double *UC);
+void orc_point_bc(const orc_params *p, int bcType, const double *UL, const double *n, double *UR);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,3 +153,32 @@ def test_operators_match_oracle(oracle):
         for d in range(mesh.nDims):
             assert np.array_equal(g.operator(1, d), o.get(f"opp_grad_spts{d}").reshape(g.nSpts, g.nSpts))
             assert np.array_equal(g.operator(2, d), o.get(f"opp_extrapolateFn{d}").reshape(g.nFpts, g.nSpts))
+
+
+GOLDEN_INVISCID = ["euler_p2_char_fixeddt", "euler_p3_char_cfl", "euler_p2_charslip_cfl", "advection_p3"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_INVISCID)
+def test_gpu_vs_reference_golden(oracle, name):
+    """The CUDA path against the reference's own outputs (tests/golden/)."""
+    import os
+
+    from fr_learn_b200 import Solver
+    from test_oracle_golden import golden_case
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_golden.npz"))
+    mesh, kw, ic, nsteps = golden_case(oracle, g, name)
+    pre = f"case/{name}/"
+    kw.pop("nDims")
+    s = Solver(mesh, **kw)
+    s.setInitialCondition(ic)
+    s.calcResidual(0)
+    assert relerr(s.get("divF_spts", 0), g[pre + "r0_divF_spts"]) < FP64_TOL
+    s2 = Solver(mesh, **kw)
+    s2.setInitialCondition(ic)
+    dts = []
+    for _ in range(nsteps):
+        s2.update(1)
+        dts.append(s2.dt)
+    assert relerr(s2.get("U_spts"), g[pre + "final_U_spts"]) < FP64_TOL
+    assert relerr(dts, g[pre + "dt_hist"]) < FP64_TOL
