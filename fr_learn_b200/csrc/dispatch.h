@@ -14,6 +14,8 @@ namespace frg {
 
 struct KernelSet {
   void (*stage)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
+  // viscous configurations: the gradient kernel launched before each stage
+  void (*grad)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
   void (*trace)(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) = nullptr;
   void (*wavesp)(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph,
                  cudaStream_t st) = nullptr;
@@ -23,7 +25,7 @@ struct KernelSet {
 };
 
 struct KernelKey {
-  int nDims, P, NV, precision, bc, riemann;
+  int nDims, P, NV, precision, bc, riemann, viscous;
 };
 
 // Fills `k` for the key, or returns false with `err` set.

@@ -177,6 +177,8 @@ struct frg_solver {
   double *U = nullptr, *U0 = nullptr, *Acc = nullptr, *divF[5] = {nullptr};
   void *W[2] = {nullptr, nullptr}, *tr[2] = {nullptr, nullptr};
   void *nrm = nullptr, *dAs = nullptr, *JG = nullptr, *detJs = nullptr;
+  void *fvn = nullptr, *fvn2 = nullptr;  // viscous: projected viscous flux per flux point
+  bool visc2 = false;                    // 3D with an LDG penalty: second projection needed
   double *detJd = nullptr, *nrmOwn = nullptr, *dAd = nullptr, *vol = nullptr, *wsurf = nullptr, *wvol = nullptr;
   int *nbr = nullptr;
   double *waveSp = nullptr, *eleDt = nullptr, *dtDev = nullptr, *timeDev = nullptr, *blockMin = nullptr;
@@ -225,6 +227,7 @@ Phys make_phys(const frg_params &p) {
   ph.gamma = p.gamma;
   ph.adv[0] = p.advectVx; ph.adv[1] = p.advectVy; ph.adv[2] = p.advectVz;
   ph.lambda = p.lambda;
+  ph.diffD = p.diffD;
   ph.rhoB = p.rhoBound; ph.vB[0] = p.uBound; ph.vB[1] = p.vBound; ph.vB[2] = p.wBound; ph.pB = p.pBound;
   ph.mu = p.mu_inf; ph.prandtl = p.prandtl; ph.c_sth = p.c_sth; ph.rt_inf = p.rt_inf;
   ph.penFact = p.penFact; ph.tau = p.tau;
@@ -294,10 +297,20 @@ StageArgs base_args(frg_solver *s) {
   a.err = s->err;
   a.vcjh = s->p.vcjhScheme;
   a.ph = make_phys(s->p);
+  a.fvnOut = s->fvn;
+  a.fvnIn = s->fvn;
+  a.fvn2Out = s->fvn2;
+  a.fvn2In = s->fvn2;
+  a.visc2 = s->visc2;
   return a;
 }
 
 frg_status launch_stage_args(frg_solver *s, StageArgs &a) {
+  if (s->ks.grad) {  // viscous: the gradient kernel first (same inputs)
+    s->ks.grad(&a, s->nBlk, s->ks.smem, s->stream);
+    frg_status st = post_launch(s);
+    if (st) return st;
+  }
   s->ks.stage(&a, s->nBlk, s->ks.smem, s->stream);
   return post_launch(s);
 }
@@ -386,7 +399,6 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   if (p.nDims != 2 && p.nDims != 3) return fail(FRG_ERR_ARG, "nDims must be 2 or 3");
   if (p.order < 1 || p.order > (p.nDims == 2 ? 5 : 4)) return fail(FRG_ERR_ARG, "order %d not supported", p.order);
   if (p.equation != 0 && p.equation != 1) return fail(FRG_ERR_ARG, "equation must be 0 or 1");
-  if (p.viscous) return fail(FRG_ERR_ARG, "viscous path not built yet");
   if (p.equation == 1 && p.riemannType == 1 && p.nDims == 3)
     return fail(FRG_ERR_ARG, "Roe not implemented in 3D");
   if (p.vcjhScheme < 0 || p.vcjhScheme > 3 || (p.vcjhScheme == 3 && p.order < 2))
@@ -411,7 +423,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   s->ops = build_ops1d(p.order, p.vcjhScheme);
   s->nS = s->g.nS; s->nF = s->g.nF; s->nE = s->g.nE;
   if ((st = upload_tables(p.nDims, p.precision))) return st;
-  KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType};
+  KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType, p.viscous ? 1 : 0};
   if (!select_kernels(key, s->ks, err)) return fail(FRG_ERR_ARG, "%s", err.c_str());
   s->sstore = p.precision == FRG_FP64 ? 8 : 4;
   s->nBlk = (s->nE + s->ks.TE - 1) / s->ks.TE;
@@ -421,6 +433,11 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   for (int i = 0; i < 2; i++) {
     if ((st = dalloc_bytes(&s->W[i], nSE * s->sstore))) return st;
     if ((st = dalloc_bytes(&s->tr[i], nFE * s->sstore))) return st;
+  }
+  if (p.viscous) {
+    s->visc2 = p.nDims == 3 && p.penFact != 0.0;
+    if ((st = dalloc_bytes(&s->fvn, nFE * s->sstore))) return st;
+    if (s->visc2 && (st = dalloc_bytes(&s->fvn2, nFE * s->sstore))) return st;
   }
   if ((st = upload_store(s.get(), &s->nrm, s->g.nrmC)) || (st = upload_store(s.get(), &s->dAs, s->g.dA)) ||
       (st = upload_store(s.get(), &s->JG, s->g.JG)) || (st = upload_store(s.get(), &s->detJs, s->g.detJ)))
@@ -497,7 +514,8 @@ frg_status frg_destroy(frg_solver *s) {
                   s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
                   s->blockMin, s->normPartial, s->normOut, s->scratchRef};
   for (double *q : dp) if (q) cudaFree(q);
-  void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->nbr, s->err, s->ticket};
+  void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->nbr, s->err, s->ticket,
+                s->fvn, s->fvn2};
   for (void *q : vp) if (q) cudaFree(q);
   cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy
   if (own) cudaStreamDestroy(own);
@@ -639,7 +657,10 @@ extern "C" {
 
 frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double *divF_dev, void *stream) {
   if (!s || !U_dev || !divF_dev) return fail(FRG_ERR_ARG, "null argument");
-  const size_t need = (size_t)s->nV * s->nF * s->nE * s->sstore;
+  // traces, and for viscous runs the projected viscous fluxes after them
+  const size_t one = (size_t)s->nV * s->nF * s->nE * s->sstore;
+  const size_t oneAligned = (one + 255) & ~size_t(255);
+  const size_t need = one + (s->ks.grad ? oneAligned * (s->visc2 ? 2 : 1) : 0);
   if (need > kNoAllocScratchBytes)
     return fail(FRG_ERR_ARG, "frg_calc_residual_noalloc: traces need %zu bytes, the scratch array holds %zu", need,
                 kNoAllocScratchBytes);
@@ -668,6 +689,16 @@ frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double 
   a.trIn = scratch;
   a.divF = divF_dev;
   a.flags = SF_RESIDUAL;
+  if (s->ks.grad) {
+    unsigned char *base = static_cast<unsigned char *>(scratch);
+    a.fvnOut = base + oneAligned;
+    a.fvnIn = a.fvnOut;
+    a.fvn2Out = s->visc2 ? base + 2 * oneAligned : nullptr;
+    a.fvn2In = a.fvn2Out;
+    s->ks.grad(&a, s->nBlk, s->ks.smem, st);
+    CK(cudaGetLastError());
+    s->launches += 1;
+  }
   s->ks.stage(&a, s->nBlk, s->ks.smem, st);
   CK(cudaGetLastError());
   s->launches += 2;
@@ -772,7 +803,7 @@ frg_status frg_update(frg_solver *s, int nsteps) {
     }
     CK(cudaGraphLaunch(ge, s->stream));
     // count the kernels the graph holds
-    s->launches += s->nRK + (s->p.dtType != 0 ? 1 + fi : 0);
+    s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? 1 + fi : 0);
     s->curTr ^= (s->nRK & 1);
   }
   if (nsteps > 0) s->divF0Valid = s->monitor;

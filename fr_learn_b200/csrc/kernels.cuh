@@ -164,142 +164,101 @@ struct StageArgs {
   unsigned *err;
   double aNext, bCur;
   int dtLocal, flags, vcjh;
+  // viscous path: this side's projected viscous flux per flux point (S),
+  // [NV][NF][nE]; the second array only for the 3D LDG penalty term
+  void *fvnOut, *fvn2Out;
+  const void *fvnIn, *fvn2In;
+  int visc2;
   Phys ph;
 };
 
 // ----------------------------------------------------------------------------
-// The fused stage kernel (inviscid Euler or scalar advection).
+// The fused stage kernels and the block-level phases they share.
 // R: arithmetic type; S: stored type of stage states, traces and metrics.
 // BC: the mesh has boundary faces (else the ghost-state code is not built);
 // RS: interior Riemann solver, 0 Rusanov, 1 Roe (boundaries always Rusanov,
-// src/face.cpp:142-145).  Two resident blocks per SM cap registers at 128.
+// src/face.cpp:142-145).
 // ----------------------------------------------------------------------------
-template <class C, typename R, typename S, bool BC, int RS>
-__global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
-  using T = Tile<C, R>;
-  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
-  R *Fs = Us + NV * NS * TE;                // [DIM][NV][NS][TE]
-  R *Js = Fs + DIM * NV * NS * TE;          // [NV][NF][TE]
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
-  const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
-  const Phys &ph = a.ph;
+
+// The state on the other side of flux point f: the neighbour's trace from the
+// previous launch's trace buffer, or the boundary ghost state.
+template <class C, typename R, typename S, bool BC>
+__device__ __forceinline__ void other_side(const StageArgs &a, int code, const R *own, const R *n, R *oth,
+                                           bool &right) {
+  constexpr int NV = C::NV, NF = C::NF, DIM = C::DIM;
+  right = false;
+  if (code >= 0) {
+    right = code & 1;
+    const size_t t = (size_t)(code >> 1);
+    const S *trIn = static_cast<const S *>(a.trIn);
+#pragma unroll
+    for (int v = 0; v < NV; v++) oth[v] = (R)trIn[(size_t)v * NF * a.nE + t];
+    return;
+  }
+  if constexpr (NV == 1 || !BC) {
+    // advection boundaries keep a zero ghost state (src/boundFace.cpp:274)
+#pragma unroll
+    for (int v = 0; v < NV; v++) oth[v] = 0;
+    if constexpr (!BC) atomicOr(a.err, ERRF_BC);
+  } else {
+    double ul[NV], ur[NV], nd[DIM];
+#pragma unroll
+    for (int v = 0; v < NV; v++) ul[v] = own[v];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) nd[d] = n[d];
+    if (!bc_ghost<DIM>(-1 - code, ul, nd, ur, a.ph)) atomicOr(a.err, ERRF_BC);
+#pragma unroll
+    for (int v = 0; v < NV; v++) oth[v] = (R)ur[v];
+  }
+}
+
+// Common inviscid flux of face::calcInviscidFlux (src/face.cpp:132-175).
+// Returns the wave speed the reference stores (negative for Roe).
+template <class C, typename R, bool BC, int RS>
+__device__ __forceinline__ R inviscid_common(const R *UL, const R *UR, const R *n, int code, R *Fn,
+                                             const Phys &ph) {
+  constexpr int NV = C::NV, DIM = C::DIM;
+  if constexpr (NV == 1) {
+    return lax_friedrichs<DIM, R>(UL[0], UR[0], n, Fn, ph);
+  } else if constexpr (RS == 0 || DIM == 3) {
+    return rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
+  } else if constexpr (BC) {
+    if (code < 0) return rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
+    roe2d<R, double>(UL, UR, n, Fn, ph);
+    return -1;
+  } else {
+    roe2d<R, double>(UL, UR, n, Fn, ph);
+    return -1;
+  }
+}
+
+// Phase A0: the tile's stage state into shared memory.
+template <class C, typename R, typename S, int TE>
+__device__ __forceinline__ void load_state(const StageArgs &a, R *Us, int e0) {
+  constexpr int NS = C::NS, NV = C::NV, NT = C::NT;
   const S *Uin_s = static_cast<const S *>(a.Uin_s);
-  const S *trIn = static_cast<const S *>(a.trIn);
-  const S *nrmG = static_cast<const S *>(a.nrm);
-  const S *dAG = static_cast<const S *>(a.dA);
-  const S *JGG = static_cast<const S *>(a.JG);
+  for (int it = threadIdx.x; it < NS * TE; it += NT) {
+    const int s = it / TE, e = it - s * TE, eg = e0 + e;
+    if (eg >= a.nE) continue;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      const size_t gi = ((size_t)v * NS + s) * a.nE + eg;
+      Us[(v * NS + s) * TE + e] = a.Uin_d ? (R)a.Uin_d[gi] : (R)Uin_s[gi];
+    }
+  }
+}
+
+// Phase C: divergence + correction (calcDivF_spts, correctDivFlux), then the
+// RK stage update in FP64 (timeStepA/B); the new state goes to Us.
+template <class C, typename R, typename S, int TE>
+__device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> &op, const R *Fs, const R *Js, R *Us,
+                                             int e0) {
+  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   const S *detJG = static_cast<const S *>(a.detJ);
   S *Wout = static_cast<S *>(a.Wout);
-  S *trOut = static_cast<S *>(a.trOut);
-
-  // ---- A: stage state and contravariant inviscid flux at solution points
-  for (int it = tid; it < NS * TE; it += NT) {
-    const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= nE) continue;
-    R u[NV];
-#pragma unroll
-    for (int v = 0; v < NV; v++) {
-      size_t gi = ((size_t)v * NS + s) * nE + eg;
-      u[v] = a.Uin_d ? (R)a.Uin_d[gi] : (R)Uin_s[gi];
-      Us[(v * NS + s) * TE + e] = u[v];
-    }
-    R F[DIM][NV];
-    inviscid_flux<DIM, NV, R>(u, F, ph);
-    R G[DIM][DIM];
-#pragma unroll
-    for (int d1 = 0; d1 < DIM; d1++)
-#pragma unroll
-      for (int d2 = 0; d2 < DIM; d2++) G[d1][d2] = (R)JGG[(((size_t)d1 * DIM + d2) * NS + s) * nE + eg];
-#pragma unroll
-    for (int d1 = 0; d1 < DIM; d1++)
-#pragma unroll
-      for (int v = 0; v < NV; v++) {
-        R t = 0;
-#pragma unroll
-        for (int d2 = 0; d2 < DIM; d2++) t += G[d1][d2] * F[d2][v];
-        Fs[((d1 * NV + v) * NS + s) * TE + e] = t;
-      }
-  }
-  __syncthreads();
-
-  // ---- B: common flux and jump at flux points
-  for (int it = tid; it < NF * TE; it += NT) {
-    const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= nE) continue;
-    int dir, side, s0, st;
-    fpt_line<C>(f, dir, side, s0, st);
-    R own[NV], dis[NV];
-#pragma unroll
-    for (int v = 0; v < NV; v++) {
-      R t = 0, q = 0;
-#pragma unroll
-      for (int j = 0; j < N1; j++) {
-        const R l = op.lag[side][j];
-        t += l * Us[(v * NS + s0 + j * st) * TE + e];
-        q += l * Fs[((dir * NV + v) * NS + s0 + j * st) * TE + e];
-      }
-      own[v] = t;
-      dis[v] = side ? q : -q;
-    }
-    R n[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; d++) n[d] = (R)nrmG[((size_t)d * NF + f) * nE + eg];
-    const R dA = (R)dAG[(size_t)f * nE + eg];
-    const int code = a.nbr[(size_t)f * nE + eg];
-    R oth[NV];
-    bool right = false;
-    int bc = 0;
-    if (code >= 0) {
-      right = code & 1;
-      const size_t t = (size_t)(code >> 1);
-#pragma unroll
-      for (int v = 0; v < NV; v++) oth[v] = (R)trIn[(size_t)v * NF * nE + t];
-    } else {
-      bc = -1 - code;
-      if constexpr (NV == 1 || !BC) {
-        // advection boundaries keep a zero ghost state (src/boundFace.cpp:274)
-#pragma unroll
-        for (int v = 0; v < NV; v++) oth[v] = 0;
-        if constexpr (!BC) atomicOr(a.err, ERRF_BC);
-      } else {
-        double ul[NV], ur[NV], nd[DIM];
-#pragma unroll
-        for (int v = 0; v < NV; v++) ul[v] = own[v];
-#pragma unroll
-        for (int d = 0; d < DIM; d++) nd[d] = n[d];
-        if (!bc_ghost<DIM>(bc, ul, nd, ur, ph)) atomicOr(a.err, ERRF_BC);
-#pragma unroll
-        for (int v = 0; v < NV; v++) oth[v] = (R)ur[v];
-      }
-    }
-    const R *UL = right ? oth : own;
-    const R *UR = right ? own : oth;
-    R Fn[NV];
-    R ws = -1;
-    if constexpr (NV == 1) {
-      ws = lax_friedrichs<DIM, R>(UL[0], UR[0], n, Fn, ph);
-    } else if constexpr (RS == 0 || DIM == 3) {
-      ws = rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
-    } else if constexpr (BC) {
-      if (code < 0) ws = rusanov<DIM, NV, R, double>(UL, UR, n, Fn, ph);
-      else roe2d<R, double>(UL, UR, n, Fn, ph);
-    } else {
-      roe2d<R, double>(UL, UR, n, Fn, ph);
-    }
-    if ((a.flags & SF_WAVESP) && !right && ws >= 0) a.waveSp[(size_t)f * nE + eg] = (double)ws;
-#pragma unroll
-    for (int v = 0; v < NV; v++) {
-      const R fo = right ? -Fn[v] * dA : Fn[v] * dA;
-      Js[(v * NF + f) * TE + e] = fo - dis[v];
-    }
-  }
-  __syncthreads();
-
-  // ---- C: divergence + correction, RK update
+  const int nE = a.nE;
   const bool resid = a.flags & SF_RESIDUAL;
-  for (int it = tid; it < NS * TE; it += NT) {
+  for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
     if (eg >= nE) continue;
     const int i = s % N1, j = (s / N1) % N1, k = DIM == 3 ? s / (N1 * N1) : 0;
@@ -350,17 +309,20 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
         }
       }
       if (last && (v == 0 || v == NV - 1) && isnan(unew)) atomicOr(a.err, ERRF_NAN);
-      Us[(v * NS + s) * TE + e] = (R)((a.flags & SF_LAST) ? unew : (double)(S)unew);
+      Us[(v * NS + s) * TE + e] = (R)(last ? unew : (double)(S)unew);
     }
   }
-  if (resid) return;
-  if ((a.flags & SF_TIME) && blockIdx.x == 0 && tid == 0) *a.time += a.dt[0];
-  __syncthreads();
+  if (!resid && (a.flags & SF_TIME) && blockIdx.x == 0 && threadIdx.x == 0) *a.time += a.dt[0];
+}
 
-  // ---- D: traces of the new state
-  for (int it = tid; it < NF * TE; it += NT) {
+// Phase D: traces of the new state for the next launch.
+template <class C, typename R, typename S, int TE>
+__device__ __forceinline__ void trace_phase(const StageArgs &a, const OpTab<R> &op, const R *Us, int e0) {
+  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1, NT = C::NT;
+  S *trOut = static_cast<S *>(a.trOut);
+  for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= nE) continue;
+    if (eg >= a.nE) continue;
     int dir, side, s0, st;
     fpt_line<C>(f, dir, side, s0, st);
 #pragma unroll
@@ -368,9 +330,465 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
       R t = 0;
 #pragma unroll
       for (int j = 0; j < N1; j++) t += op.lag[side][j] * Us[(v * NS + s0 + j * st) * TE + e];
-      trOut[((size_t)v * NF + f) * nE + eg] = (S)t;
+      trOut[((size_t)v * NF + f) * a.nE + eg] = (S)t;
     }
   }
+}
+
+// Own trace of every field at flux point f: sum over the coordinate line.
+template <class C, typename R, int TE>
+__device__ __forceinline__ void own_trace(const OpTab<R> &op, const R *Us, int f, int e, R *out) {
+  int dir, side, s0, st;
+  fpt_line<C>(f, dir, side, s0, st);
+#pragma unroll
+  for (int v = 0; v < C::NV; v++) {
+    R t = 0;
+#pragma unroll
+    for (int j = 0; j < C::N1; j++) t += op.lag[side][j] * Us[(v * C::NS + s0 + j * st) * TE + e];
+    out[v] = t;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Inviscid stage kernel (Euler or scalar advection).  Two resident blocks
+// per SM cap registers at 128.
+// ----------------------------------------------------------------------------
+template <class C, typename R, typename S, bool BC, int RS>
+__global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
+  using T = Tile<C, R>;
+  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
+  R *Fs = Us + NV * NS * TE;                // [DIM][NV][NS][TE]
+  R *Js = Fs + DIM * NV * NS * TE;          // [NV][NF][TE]
+  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
+  const Phys &ph = a.ph;
+  const S *nrmG = static_cast<const S *>(a.nrm);
+  const S *dAG = static_cast<const S *>(a.dA);
+  const S *JGG = static_cast<const S *>(a.JG);
+
+  // ---- A: stage state and contravariant inviscid flux at solution points
+  load_state<C, R, S, TE>(a, Us, e0);
+  __syncthreads();
+  for (int it = tid; it < NS * TE; it += NT) {
+    const int s = it / TE, e = it - s * TE, eg = e0 + e;
+    if (eg >= nE) continue;
+    R u[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) u[v] = Us[(v * NS + s) * TE + e];
+    R F[DIM][NV];
+    inviscid_flux<DIM, NV, R>(u, F, ph);
+    R G[DIM][DIM];
+#pragma unroll
+    for (int d1 = 0; d1 < DIM; d1++)
+#pragma unroll
+      for (int d2 = 0; d2 < DIM; d2++) G[d1][d2] = (R)JGG[(((size_t)d1 * DIM + d2) * NS + s) * nE + eg];
+#pragma unroll
+    for (int d1 = 0; d1 < DIM; d1++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        R t = 0;
+#pragma unroll
+        for (int d2 = 0; d2 < DIM; d2++) t += G[d1][d2] * F[d2][v];
+        Fs[((d1 * NV + v) * NS + s) * TE + e] = t;
+      }
+  }
+  __syncthreads();
+
+  // ---- B: common flux and jump at flux points
+  for (int it = tid; it < NF * TE; it += NT) {
+    const int f = it / TE, e = it - f * TE, eg = e0 + e;
+    if (eg >= nE) continue;
+    int dir, side, s0, st;
+    fpt_line<C>(f, dir, side, s0, st);
+    R own[NV], dis[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      R t = 0, q = 0;
+#pragma unroll
+      for (int j = 0; j < N1; j++) {
+        const R l = op.lag[side][j];
+        t += l * Us[(v * NS + s0 + j * st) * TE + e];
+        q += l * Fs[((dir * NV + v) * NS + s0 + j * st) * TE + e];
+      }
+      own[v] = t;
+      dis[v] = side ? q : -q;
+    }
+    R n[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) n[d] = (R)nrmG[((size_t)d * NF + f) * nE + eg];
+    const R dA = (R)dAG[(size_t)f * nE + eg];
+    const int code = a.nbr[(size_t)f * nE + eg];
+    R oth[NV];
+    bool right;
+    other_side<C, R, S, BC>(a, code, own, n, oth, right);
+    const R *UL = right ? oth : own;
+    const R *UR = right ? own : oth;
+    R Fn[NV];
+    const R ws = inviscid_common<C, R, BC, RS>(UL, UR, n, code, Fn, ph);
+    if ((a.flags & SF_WAVESP) && !right && ws >= 0) a.waveSp[(size_t)f * nE + eg] = (double)ws;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      const R fo = right ? -Fn[v] * dA : Fn[v] * dA;
+      Js[(v * NF + f) * TE + e] = fo - dis[v];
+    }
+  }
+  __syncthreads();
+
+  // ---- C: divergence + correction, RK update
+  update_phase<C, R, S, TE>(a, op, Fs, Js, Us, e0);
+  if (a.flags & SF_RESIDUAL) return;
+  __syncthreads();
+
+  // ---- D: traces of the new state
+  trace_phase<C, R, S, TE>(a, op, Us, e0);
+}
+
+// ----------------------------------------------------------------------------
+// Viscous path (solver::calcResidual with viscous = 1, src/solver.cpp:252-291):
+// two launches per RK stage.
+//   fr_visc_grad_kernel   LDG common solution, corrected physical gradient,
+//                         and, per flux point, the viscous flux of this side
+//                         projected on the face normal (what the other side
+//                         of the face needs from it);
+//   fr_stage_visc_kernel  recomputes the gradient locally (cheaper than a
+//                         round trip through HBM), then fluxes, common
+//                         inviscid + LDG viscous flux, divergence,
+//                         correction, RK update and traces.
+// ----------------------------------------------------------------------------
+
+// Elements per block for the viscous kernels (state, jumps, gradient, flux).
+template <class C, typename R>
+struct TileV {
+  static constexpr int PER_ELE = (C::NV * C::NS + C::NV * C::NF + 2 * C::DIM * C::NV * C::NS) * (int)sizeof(R);
+  static constexpr int TE = (32 * PER_ELE <= 100 * 1024) ? 32 : (16 * PER_ELE <= 100 * 1024) ? 16
+                            : (8 * PER_ELE <= 110 * 1024) ? 8 : 4;
+  static constexpr int SMEM = TE * PER_ELE;
+};
+
+// Normal direction of the c-th face (faces in reference order).
+template <class C>
+__device__ __forceinline__ int face_dir(int c) {
+  if constexpr (C::DIM == 2) return (c & 1) ? 0 : 1;
+  else return c < 2 ? 2 : (c < 4 ? 0 : 1);
+}
+
+// LDG penalty sign: face::ldgSolution (src/face.cpp:590-598).
+template <int DIM, typename R>
+__device__ __forceinline__ R ldg_pen(const R *n, double penFact) {
+  if constexpr (DIM == 2) return (n[0] + n[1] < (R)0) ? (R)-penFact : (R)penFact;
+  else return (n[0] + n[1] + (R)1.4142135623730951 * n[2] < (R)0) ? (R)-penFact : (R)penFact;
+}
+
+// B1: common solution minus own trace at every flux point (ldgSolution, and
+// dUc = UC - U of face::calcInviscidFlux / intFace::setRightStateSolution).
+template <class C, typename R, typename S, bool BC, int TE>
+__device__ __forceinline__ void ldg_phase(const StageArgs &a, const OpTab<R> &op, const R *Us, R *Dc, int e0) {
+  constexpr int NF = C::NF, NV = C::NV, DIM = C::DIM, NT = C::NT;
+  const S *nrmG = static_cast<const S *>(a.nrm);
+  for (int it = threadIdx.x; it < NF * TE; it += NT) {
+    const int f = it / TE, e = it - f * TE, eg = e0 + e;
+    if (eg >= a.nE) continue;
+    R own[NV], oth[NV], n[DIM];
+    own_trace<C, R, TE>(op, Us, f, e, own);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) n[d] = (R)nrmG[((size_t)d * NF + f) * a.nE + eg];
+    const int code = a.nbr[(size_t)f * a.nE + eg];
+    bool right;
+    other_side<C, R, S, BC>(a, code, own, n, oth, right);
+    const R *UL = right ? oth : own;
+    const R *UR = right ? own : oth;
+    const R pf = code < 0 ? (R)0 : ldg_pen<DIM, R>(n, a.ph.penFact);
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      const R uc = code < 0 ? (R)0.5 * (UL[v] + UR[v]) : (R)0.5 * (UL[v] + UR[v]) - pf * (UL[v] - UR[v]);
+      Dc[(v * NF + f) * TE + e] = uc - own[v];
+    }
+  }
+}
+
+// C1: physical gradient at solution points: D U + correction by the common
+// solution (calcGradU_spts, correctGradU src/solver.cpp:808-879), then
+// JGinv^T / detJ.  dUs is [DIM][NV][NS][TE].
+template <class C, typename R, typename S, int TE>
+__device__ __forceinline__ void gradient_phase(const StageArgs &a, const OpTab<R> &op, const R *Us, const R *Dc,
+                                               R *dUs, int e0) {
+  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  const S *JGG = static_cast<const S *>(a.JG);
+  const S *detJG = static_cast<const S *>(a.detJ);
+  for (int it = threadIdx.x; it < NS * TE; it += NT) {
+    const int s = it / TE, e = it - s * TE, eg = e0 + e;
+    if (eg >= a.nE) continue;
+    const int i = s % N1, j = (s / N1) % N1, k = DIM == 3 ? s / (N1 * N1) : 0;
+    const int ijk[3] = {i, j, k};
+    int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
+    corr_fpts<C>(i, j, k, cf, cs, ca);
+    R G[DIM][DIM];
+#pragma unroll
+    for (int d1 = 0; d1 < DIM; d1++)
+#pragma unroll
+      for (int d2 = 0; d2 < DIM; d2++) G[d1][d2] = (R)JGG[(((size_t)d1 * DIM + d2) * NS + s) * a.nE + eg];
+    const R invDet = (R)1. / (R)detJG[(size_t)s * a.nE + eg];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      R gr[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        const int sd = d == 0 ? 1 : d == 1 ? N1 : N1 * N1;
+        const int sb = s - ijk[d] * sd;
+        R acc = 0;
+#pragma unroll
+        for (int q = 0; q < N1; q++) acc += op.dlag[ijk[d]][q] * Us[(v * NS + sb + q * sd) * TE + e];
+#pragma unroll
+        for (int c = 0; c < 2 * DIM; c++)
+          if (face_dir<C>(c) == d) acc += (cs[c] ? op.gR[ca[c]] : op.gL[ca[c]]) * Dc[(v * NF + cf[c]) * TE + e];
+        gr[d] = acc;
+      }
+#pragma unroll
+      for (int d1 = 0; d1 < DIM; d1++) {
+        R t = 0;
+#pragma unroll
+        for (int d2 = 0; d2 < DIM; d2++) t += gr[d2] * G[d2][d1];
+        dUs[((d1 * NV + v) * NS + s) * TE + e] = invDet * t;
+      }
+    }
+  }
+}
+
+// Gradient trace [DIM][NV] at own flux point f (extrapolateGradU, :881-895).
+template <class C, typename R, int TE>
+__device__ __forceinline__ void own_grad_trace(const OpTab<R> &op, const R *dUs, int f, int e, R *g) {
+  int dir, side, s0, st;
+  fpt_line<C>(f, dir, side, s0, st);
+#pragma unroll
+  for (int q = 0; q < C::DIM * C::NV; q++) {
+    R t = 0;
+#pragma unroll
+    for (int j = 0; j < C::N1; j++) t += op.lag[side][j] * dUs[(q * C::NS + s0 + j * st) * TE + e];
+    g[q] = t;
+  }
+}
+
+// Viscous flux [DIM][NV] of a state and its physical gradient.
+template <class C, typename R>
+__device__ __forceinline__ void visc_flux(const R *u, const R *g, R Fv[C::DIM][C::NV], const Phys &ph) {
+  if constexpr (C::NV == 1) {
+    R t[C::DIM][1];
+    viscous_flux_ad<C::DIM, R>(g, t, ph);
+#pragma unroll
+    for (int d = 0; d < C::DIM; d++) Fv[d][0] = t[d][0];
+  } else {
+    viscous_flux<C::DIM, R>(u, g, Fv, ph);
+  }
+}
+
+template <class C, typename R, typename S, bool BC>
+__global__ void __launch_bounds__(C::NT, 1) fr_visc_grad_kernel(const StageArgs a) {
+  using T = TileV<C, R>;
+  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, NT = C::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
+  R *Dc = Us + NV * NS * TE;                // [NV][NF][TE]
+  R *dUs = Dc + NV * NF * TE;               // [DIM][NV][NS][TE]
+  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const int e0 = blockIdx.x * TE;
+  const S *nrmG = static_cast<const S *>(a.nrm);
+  S *fvnOut = static_cast<S *>(a.fvnOut);
+  S *fvn2Out = static_cast<S *>(a.fvn2Out);
+  load_state<C, R, S, TE>(a, Us, e0);
+  __syncthreads();
+  ldg_phase<C, R, S, BC, TE>(a, op, Us, Dc, e0);
+  __syncthreads();
+  gradient_phase<C, R, S, TE>(a, op, Us, Dc, dUs, e0);
+  __syncthreads();
+  // this side's viscous flux, projected, at every interior flux point
+  for (int it = threadIdx.x; it < NF * TE; it += NT) {
+    const int f = it / TE, e = it - f * TE, eg = e0 + e;
+    if (eg >= a.nE || a.nbr[(size_t)f * a.nE + eg] < 0) continue;
+    R u[NV], g[DIM * NV], n[DIM], Fv[DIM][NV];
+    own_trace<C, R, TE>(op, Us, f, e, u);
+    own_grad_trace<C, R, TE>(op, dUs, f, e, g);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) n[d] = (R)nrmG[((size_t)d * NF + f) * a.nE + eg];
+    visc_flux<C, R>(u, g, Fv, a.ph);
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      R fn = 0;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) fn += Fv[d][v] * n[d];
+      fvnOut[((size_t)v * NF + f) * a.nE + eg] = (S)fn;
+      if constexpr (DIM == 3) {
+        // the LDG penalty term of the reference reads FL[1] where FL[2] is
+        // meant (src/face.cpp:245): the left side contributes n0 F0 + n1 F1 + n2 F1
+        if (a.visc2) fvn2Out[((size_t)v * NF + f) * a.nE + eg] = (S)(n[0] * Fv[0][v] + n[1] * Fv[1][v] + n[2] * Fv[1][v]);
+      }
+    }
+  }
+}
+
+template <class C, typename R, typename S, bool BC, int RS>
+__global__ void __launch_bounds__(C::NT, 1) fr_stage_visc_kernel(const StageArgs a) {
+  using T = TileV<C, R>;
+  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
+  R *Js = Us + NV * NS * TE;                // [NV][NF][TE]: dUc, then the jumps
+  R *dUs = Js + NV * NF * TE;               // [DIM][NV][NS][TE]
+  R *Fs = dUs + DIM * NV * NS * TE;         // [DIM][NV][NS][TE]
+  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
+  const Phys &ph = a.ph;
+  const S *nrmG = static_cast<const S *>(a.nrm);
+  const S *dAG = static_cast<const S *>(a.dA);
+  const S *JGG = static_cast<const S *>(a.JG);
+  const S *fvnIn = static_cast<const S *>(a.fvnIn);
+  const S *fvn2In = static_cast<const S *>(a.fvn2In);
+
+  load_state<C, R, S, TE>(a, Us, e0);
+  __syncthreads();
+  ldg_phase<C, R, S, BC, TE>(a, op, Us, Js, e0);
+  __syncthreads();
+  gradient_phase<C, R, S, TE>(a, op, Us, Js, dUs, e0);
+  __syncthreads();
+
+  // ---- A: inviscid + viscous flux at solution points, transformed
+  // (calcInviscidFlux_spts keeps the physical flux, calcViscousFlux_spts
+  //  src/solver.cpp:562-596 adds the viscous flux and applies JGinv)
+  for (int it = tid; it < NS * TE; it += NT) {
+    const int s = it / TE, e = it - s * TE, eg = e0 + e;
+    if (eg >= nE) continue;
+    R u[NV], g[DIM * NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) u[v] = Us[(v * NS + s) * TE + e];
+#pragma unroll
+    for (int q = 0; q < DIM * NV; q++) g[q] = dUs[(q * NS + s) * TE + e];
+    R Fi[DIM][NV], Fv[DIM][NV];
+    inviscid_flux<DIM, NV, R>(u, Fi, ph);
+    visc_flux<C, R>(u, g, Fv, ph);
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) Fv[d][v] += Fi[d][v];
+    R G[DIM][DIM];
+#pragma unroll
+    for (int d1 = 0; d1 < DIM; d1++)
+#pragma unroll
+      for (int d2 = 0; d2 < DIM; d2++) G[d1][d2] = (R)JGG[(((size_t)d1 * DIM + d2) * NS + s) * nE + eg];
+#pragma unroll
+    for (int d1 = 0; d1 < DIM; d1++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        R t = 0;
+#pragma unroll
+        for (int d2 = 0; d2 < DIM; d2++) t += G[d1][d2] * Fv[d2][v];
+        Fs[((d1 * NV + v) * NS + s) * TE + e] = t;
+      }
+  }
+  __syncthreads();
+
+  // ---- B: common inviscid + LDG viscous flux (face::calcInviscidFlux and
+  // face::calcViscousFlux, src/face.cpp:132-287) and the jumps
+  for (int it = tid; it < NF * TE; it += NT) {
+    const int f = it / TE, e = it - f * TE, eg = e0 + e;
+    if (eg >= nE) continue;
+    int dir, side, s0, st;
+    fpt_line<C>(f, dir, side, s0, st);
+    R own[NV], dis[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      R t = 0, q = 0;
+#pragma unroll
+      for (int j = 0; j < N1; j++) {
+        const R l = op.lag[side][j];
+        t += l * Us[(v * NS + s0 + j * st) * TE + e];
+        q += l * Fs[((dir * NV + v) * NS + s0 + j * st) * TE + e];
+      }
+      own[v] = t;
+      dis[v] = side ? q : -q;
+    }
+    R n[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) n[d] = (R)nrmG[((size_t)d * NF + f) * nE + eg];
+    const R dA = (R)dAG[(size_t)f * nE + eg];
+    const int code = a.nbr[(size_t)f * nE + eg];
+    R oth[NV];
+    bool right;
+    other_side<C, R, S, BC>(a, code, own, n, oth, right);
+    const R *UL = right ? oth : own;
+    const R *UR = right ? own : oth;
+    R Fn[NV];
+    const R ws = inviscid_common<C, R, BC, RS>(UL, UR, n, code, Fn, ph);
+    if ((a.flags & SF_WAVESP) && !right && ws >= 0) a.waveSp[(size_t)f * nE + eg] = (double)ws;
+    // this side's viscous flux at the flux point
+    R g[DIM * NV], Fo[DIM][NV];
+    own_grad_trace<C, R, TE>(op, dUs, f, e, g);
+    visc_flux<C, R>(own, g, Fo, ph);
+    R nn = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) nn += n[d] * n[d];
+    const R tau = (R)ph.tau;
+    if (code >= 0) {
+      const size_t t = (size_t)(code >> 1);
+      const R pf = ldg_pen<DIM, R>(n, ph.penFact);
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        R on = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) on += Fo[d][v] * n[d];
+        const R xn = (R)fvnIn[(size_t)v * NF * nE + t];
+        const R FLn = right ? xn : on, FRn = right ? on : xn;
+        if constexpr (NV == 1) {
+          Fn[v] += (R)0.5 * (FLn + FRn);  // centralFlux (src/flux.cpp:379-387)
+        } else {
+          R jumpF = FLn - FRn;
+          if constexpr (DIM == 3) {
+            const R al = right ? (a.visc2 ? (R)fvn2In[(size_t)v * NF * nE + t] : xn)
+                               : n[0] * Fo[0][v] + n[1] * Fo[1][v] + n[2] * Fo[1][v];
+            jumpF = al - FRn;
+          }
+          Fn[v] += (R)0.5 * (FLn + FRn) + pf * nn * jumpF + tau * nn * (UL[v] - UR[v]);
+        }
+      }
+    } else {
+      if constexpr (NV == 1) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) Fn[0] += (R)0.5 * Fo[d][0] * n[d];  // ghost gradient is zero
+      } else {
+        if constexpr (BC) {
+          R Fb[DIM][NV];
+          if (-1 - code == BC_ADI_NOSLIP) {
+            R gR[DIM * NV];
+            adiabatic_gradient<DIM, R>(UL, UR, g, gR, ph);
+            visc_flux<C, R>(UR, gR, Fb, ph);
+          } else {
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+#pragma unroll
+              for (int v = 0; v < NV; v++) Fb[d][v] = Fo[d][v];
+          }
+#pragma unroll
+          for (int v = 0; v < NV; v++) {
+            R bn = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) bn += Fb[d][v] * n[d];
+            Fn[v] += bn + tau * nn * (UL[v] - UR[v]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      const R fo = right ? -Fn[v] * dA : Fn[v] * dA;
+      Js[(v * NF + f) * TE + e] = fo - dis[v];
+    }
+  }
+  __syncthreads();
+
+  update_phase<C, R, S, TE>(a, op, Fs, Js, Us, e0);
+  if (a.flags & SF_RESIDUAL) return;
+  __syncthreads();
+  trace_phase<C, R, S, TE>(a, op, Us, e0);
 }
 
 // ----------------------------------------------------------------------------

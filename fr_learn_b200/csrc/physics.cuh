@@ -18,6 +18,7 @@ struct Phys {
   double gamma;
   double adv[3];  // advectVx, advectVy, advectVz
   double lambda;  // Lax-Friedrichs upwinding factor
+  double diffD;   // advection-diffusion coefficient
   double rhoB, vB[3], pB;
   double mu, prandtl, c_sth, rt_inf;
   double penFact, tau;
@@ -152,6 +153,107 @@ __device__ __forceinline__ R lax_friedrichs(R uL, R uR, const R *n, R *Fn, const
   if constexpr (DIM == 3) vN += (R)ph.adv[2] * n[2];
   Fn[0] = vN * uAvg + (R)0.5 * (R)ph.lambda * fabs(vN) * uDiff;
   return fabs(vN);
+}
+
+// viscousFlux (src/flux.cpp:90-226), Navier-Stokes, with the reference's
+// index slips kept: tauxz = mu(du/dz + dv/dx), tauyz = mu(du/dz + dv/dy)
+// (:197-198) and Fvis[0][3] = -tauzz, Fvis[1][3] = -tauyz (:216-217).
+// g is the physical gradient [DIM][NV].
+template <int DIM, typename R>
+__device__ __forceinline__ void viscous_flux(const R *U, const R *g, R Fv[DIM][DIM + 2], const Phys &ph) {
+  constexpr int NV = DIM + 2;
+  auto G = [&](int a, int b) { return g[a * NV + b]; };
+  R rho = U[0], u = U[1] / rho, v = U[2] / rho;
+  R e = U[DIM + 1] / rho - (R)0.5 * (u * u + v * v);
+  R w = 0;
+  if constexpr (DIM == 3) {
+    w = U[3] / rho;
+    e -= (R)0.5 * (w * w);
+  }
+  R dRho_dx = G(0, 0), dRhoU_dx = G(0, 1), dRhoV_dx = G(0, 2), dE_dx = G(0, DIM + 1);
+  R dRho_dy = G(1, 0), dRhoU_dy = G(1, 1), dRhoV_dy = G(1, 2), dE_dy = G(1, DIM + 1);
+  R dRho_dz = 0, dRhoU_dz = 0, dRhoW_dx = 0, dRhoW_dy = 0, dRhoW_dz = 0, dE_dz = 0;
+  if constexpr (DIM == 3) {
+    dRho_dz = G(2, 0); dRhoU_dz = G(2, 1);
+    dRhoW_dx = G(0, 3); dRhoW_dy = G(1, 3); dRhoW_dz = G(2, 3); dE_dz = G(2, 4);
+  }
+  R mu = (R)ph.mu;
+  if (!ph.fixVis) {  // Sutherland's law
+    R rt = ((R)ph.gamma - (R)1.0) * e / (R)ph.rt_inf;
+    mu *= pow(rt, (R)1.5) * ((R)1. + (R)ph.c_sth) / (rt + (R)ph.c_sth);
+  }
+  R du_dx = (dRhoU_dx - dRho_dx * u) / rho, du_dy = (dRhoU_dy - dRho_dy * u) / rho;
+  R dv_dx = (dRhoV_dx - dRho_dx * v) / rho, dv_dy = (dRhoV_dy - dRho_dy * v) / rho;
+  R du_dz = 0, dw_dx = 0, dw_dy = 0, dw_dz = 0;
+  if constexpr (DIM == 3) {
+    du_dz = (dRhoU_dz - dRho_dz * u) / rho;
+    dw_dx = (dRhoW_dx - dRho_dx * w) / rho;
+    dw_dy = (dRhoW_dy - dRho_dy * w) / rho;
+    dw_dz = (dRhoW_dz - dRho_dz * w) / rho;
+  }
+  R dK_dx, dK_dy, dK_dz = 0;
+  if constexpr (DIM == 2) {
+    dK_dx = (R)0.5 * (u * u + v * v) * dRho_dx + rho * (u * du_dx + v * dv_dx);
+    dK_dy = (R)0.5 * (u * u + v * v) * dRho_dy + rho * (u * du_dy + v * dv_dy);
+  } else {
+    // the reference also forms dv/dz here; it only enters dK_dz
+    R dv_dz = (G(2, 2) - dRho_dz * v) / rho;
+    dK_dx = (R)0.5 * (u * u + v * v + w * w) * dRho_dx + rho * (u * du_dx + v * dv_dx + w * dw_dx);
+    dK_dy = (R)0.5 * (u * u + v * v + w * w) * dRho_dy + rho * (u * du_dy + v * dv_dy + w * dw_dy);
+    dK_dz = (R)0.5 * (u * u + v * v + w * w) * dRho_dz + rho * (u * du_dz + v * dv_dz + w * dw_dz);
+  }
+  R de_dx = (dE_dx - dK_dx - dRho_dx * e) / rho;
+  R de_dy = (dE_dy - dK_dy - dRho_dy * e) / rho;
+  R de_dz = 0;
+  if constexpr (DIM == 3) de_dz = (dE_dz - dK_dz - dRho_dz * e) / rho;
+  R diag = (du_dx + dv_dy + dw_dz) / (R)3.0;
+  R tauxx = (R)2.0 * mu * (du_dx - diag), tauyy = (R)2.0 * mu * (dv_dy - diag);
+  R tauxy = mu * (du_dy + dv_dx);
+  R tauxz = 0, tauyz = 0, tauzz = 0;
+  if constexpr (DIM == 3) {
+    tauxz = mu * (du_dz + dv_dx);
+    tauyz = mu * (du_dz + dv_dy);
+    tauzz = (R)2.0 * mu * (dw_dz - diag);
+  }
+  const R kap = (mu / (R)ph.prandtl) * (R)ph.gamma;
+  Fv[0][0] = 0; Fv[0][1] = -tauxx; Fv[0][2] = -tauxy;
+  Fv[0][DIM + 1] = -(u * tauxx + v * tauxy + w * tauxz + kap * de_dx);
+  Fv[1][0] = 0; Fv[1][1] = -tauxy; Fv[1][2] = -tauyy;
+  Fv[1][DIM + 1] = -(u * tauxy + v * tauyy + w * tauyz + kap * de_dy);
+  if constexpr (DIM == 3) {
+    Fv[0][3] = -tauzz; Fv[1][3] = -tauyz;
+    Fv[2][0] = 0; Fv[2][1] = -tauxz; Fv[2][2] = -tauyz; Fv[2][3] = -tauzz;
+    Fv[2][4] = -(u * tauxz + v * tauyz + w * tauzz + kap * de_dz);
+  }
+}
+
+// viscousFluxAD (src/flux.cpp:361-366): -D grad u.
+template <int DIM, typename R>
+__device__ __forceinline__ void viscous_flux_ad(const R *g, R Fv[DIM][1], const Phys &ph) {
+#pragma unroll
+  for (int d = 0; d < DIM; d++) Fv[d][0] = -(R)ph.diffD * g[d];
+}
+
+// boundFace::applyViscousBCs, adiabatic no-slip wall (src/boundFace.cpp:279-320):
+// the ghost gradient is the interior one with its energy row rebuilt so the
+// temperature gradient vanishes.  gL, gR are [DIM][NV].
+template <int DIM, typename R>
+__device__ __forceinline__ void adiabatic_gradient(const R *UL, const R *UR, const R *gL, R *gR, const Phys &ph) {
+  constexpr int NV = DIM + 2;
+  for (int i = 0; i < DIM * NV; i++) gR[i] = gL[i];
+  R rhovSq = 0;
+  for (int d = 0; d < DIM; d++) rhovSq += UL[d + 1] * UL[d + 1];
+  R pL = ((R)ph.gamma - (R)1.) * (UL[DIM + 1] - (R)0.5 * rhovSq / UL[0]);
+  R e = pL / (((R)ph.gamma - (R)1.) * UR[0]);
+  R gv[DIM][DIM];
+  for (int a = 0; a < DIM; a++)
+    for (int b = 0; b < DIM; b++) gv[a][b] = (gR[a * NV + b + 1] - gR[a * NV] * UR[b + 1] / UR[0]) / UR[0];
+  R vSq = 0;
+  for (int d = 0; d < DIM; d++) vSq += UR[d + 1] * UR[d + 1] / (UR[0] * UR[0]);
+  for (int a = 0; a < DIM; a++) {
+    gR[a * NV + DIM + 1] = (e + (R)0.5 * vSq) * gR[a * NV];
+    for (int b = 0; b < DIM; b++) gR[a * NV + DIM + 1] += UR[b + 1] * gv[b][a];
+  }
 }
 
 // boundFace::applyBCs for Euler/Navier-Stokes (src/boundFace.cpp:33-277),

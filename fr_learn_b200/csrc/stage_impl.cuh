@@ -13,6 +13,14 @@ template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_stage_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
 }
+template <class C, typename R, typename S, bool BC, int RS>
+void launch_stage_visc(const void *args, int nBlk, size_t smem, cudaStream_t st) {
+  fr_stage_visc_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
+}
+template <class C, typename R, typename S, bool BC>
+void launch_grad(const void *args, int nBlk, size_t smem, cudaStream_t st) {
+  fr_visc_grad_kernel<C, R, S, BC><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
+}
 template <class C, typename R, typename S>
 void launch_trace(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) {
   long n = (long)C::NF * nE;
@@ -42,15 +50,42 @@ bool make_set(KernelSet &k, std::string &err) {
   return true;
 }
 
+template <class C, typename R, typename S, bool BC, int RS>
+bool make_set_visc(KernelSet &k, std::string &err) {
+  using T = TileV<C, R>;
+  k.stage = &launch_stage_visc<C, R, S, BC, RS>;
+  k.grad = &launch_grad<C, R, S, BC>;
+  k.trace = &launch_trace<C, R, S>;
+  k.wavesp = &launch_wavesp<C::DIM, C::NV, S>;
+  k.TE = T::TE;
+  k.NT = C::NT;
+  k.smem = T::SMEM;
+  auto f1 = fr_stage_visc_kernel<C, R, S, BC, RS>;
+  auto f2 = fr_visc_grad_kernel<C, R, S, BC>;
+  cudaError_t e = cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(f1, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(f2, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
+template <class C, typename R, typename S, bool BC, int RS>
+bool make_one(const KernelKey &key, KernelSet &k, std::string &err) {
+  return key.viscous ? make_set_visc<C, R, S, BC, RS>(k, err) : make_set<C, R, S, BC, RS>(k, err);
+}
+
 template <int DIM, int P, int NV, typename R, typename S>
 bool make_variant(const KernelKey &key, KernelSet &k, std::string &err) {
   using C = Cfg<DIM, P, NV>;
   if constexpr (NV == 1 || DIM == 3) {
-    return key.bc ? make_set<C, R, S, true, 0>(k, err) : make_set<C, R, S, false, 0>(k, err);
+    return key.bc ? make_one<C, R, S, true, 0>(key, k, err) : make_one<C, R, S, false, 0>(key, k, err);
   } else {
     if (key.riemann == 1)
-      return key.bc ? make_set<C, R, S, true, 1>(k, err) : make_set<C, R, S, false, 1>(k, err);
-    return key.bc ? make_set<C, R, S, true, 0>(k, err) : make_set<C, R, S, false, 0>(k, err);
+      return key.bc ? make_one<C, R, S, true, 1>(key, k, err) : make_one<C, R, S, false, 1>(key, k, err);
+    return key.bc ? make_one<C, R, S, true, 0>(key, k, err) : make_one<C, R, S, false, 0>(key, k, err);
   }
 }
 

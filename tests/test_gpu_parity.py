@@ -47,6 +47,24 @@ def cases():
                                 dict(order=3, dtType=0, dt=1e-3)),
         "advection3d_p2": (box3d(3, 3, 3, (-2, -2, -2), (2, 2, 2), bcs=char6), 0,
                            dict(order=2, equation=0, dtType=1, CFL=0.3)),
+        # viscous (LDG) cases
+        "ns2d_p3_roe_ldg": (box2d(6, 6, -10, 10, -10, 10, perturb=0.1, seed=12), 1,
+                            dict(order=3, riemannType=1, viscous=1, mu_inf=0.01, prandtl=0.72, fixVis=1,
+                                 penFact=0.5, tau=1.0, dtType=1, CFL=0.3)),
+        "ns2d_p4_sutherland": (box2d(5, 4, -10, 10, -10, 10, perturb=0.1, seed=13), 1,
+                               dict(order=4, riemannType=0, viscous=1, mu_inf=0.02, prandtl=0.71, fixVis=0,
+                                    c_sth=0.41, rt_inf=2.5, penFact=0.0, tau=1.0, dtType=0, dt=1e-3)),
+        "tgv3d_p3": (box3d(3, 3, 3, (0, 0, 0), (2 * np.pi,) * 3, perturb=0.05, seed=14), 10,
+                     dict(order=3, viscous=1, mu_inf=1.0 / 1600, prandtl=0.71, fixVis=1, penFact=0.0, tau=1.0,
+                          dtType=0, dt=1e-3)),
+        "ns3d_p2_penalty_walls": (box3d(3, 3, 3, (-2, -2, -1), (2, 2, 1),
+                                        bcs={"zmin": "adiabatic_noslip", "zmax": "isothermal_noslip"},
+                                        perturb=0.1, seed=15), 1,
+                                  dict(order=2, viscous=1, mu_inf=0.01, prandtl=0.72, fixVis=1, penFact=0.3,
+                                       tau=1.0, TWall=1.0, RGas=1.0 / 1.4, dtType=1, CFL=0.3)),
+        "advdiff2d_p3": (box2d(6, 6, perturb=0.1, seed=16), 0,
+                         dict(order=3, equation=0, viscous=1, diffD=0.05, penFact=0.2, tau=1.0, dtType=0,
+                              dt=1e-3)),
     }
 
 
@@ -155,7 +173,8 @@ def test_operators_match_oracle(oracle):
             assert np.array_equal(g.operator(2, d), o.get(f"opp_extrapolateFn{d}").reshape(g.nFpts, g.nSpts))
 
 
-GOLDEN_INVISCID = ["euler_p2_char_fixeddt", "euler_p3_char_cfl", "euler_p2_charslip_cfl", "advection_p3"]
+GOLDEN_INVISCID = ["euler_p2_char_fixeddt", "euler_p3_char_cfl", "euler_p2_charslip_cfl", "advection_p3",
+                   "ns_p2_sutherland_ldg", "ns_p3_walls"]
 
 
 @pytest.mark.parametrize("name", GOLDEN_INVISCID)
