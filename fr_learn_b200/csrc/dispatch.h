@@ -16,7 +16,9 @@ struct KernelSet {
   void (*stage)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
   // viscous configurations: the gradient kernel launched before each stage
   void (*grad)(const void *args, int nBlk, size_t smem, cudaStream_t st) = nullptr;
-  void (*trace)(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) = nullptr;
+  // traces of a double state: nE is the element stride of the trace array,
+  // nEle the number of real elements, ldU the element stride of U
+  void (*trace)(const double *U, void *tr, int nE, int nEle, int ldU, int vcjh, cudaStream_t st) = nullptr;
   void (*wavesp)(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph,
                  cudaStream_t st) = nullptr;
   int TE = 0;       // elements per block

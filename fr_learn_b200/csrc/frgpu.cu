@@ -22,7 +22,7 @@ namespace frg {
 // ----------------------------------------------------------------- kernels
 __global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__restrict__ dA,
                              const double *__restrict__ vol, const double *__restrict__ wsurf, int NF, int NFF,
-                             int nE, double cflFac, double *eleDt, double *blockMin, unsigned *ticket,
+                             int nE, int L, double cflFac, double *eleDt, double *blockMin, unsigned *ticket,
                              double *dtOut, unsigned *err) {
   __shared__ double wmin[32];
   __shared__ bool last;
@@ -30,7 +30,7 @@ __global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__
   double my = INFINITY;
   if (e < nE) {
     double iw = 0;
-    for (int f = 0; f < NF; f++) iw += waveSp[(size_t)f * nE + e] * wsurf[f % NFF] * dA[(size_t)f * nE + e];
+    for (int f = 0; f < NF; f++) iw += waveSp[(size_t)f * L + e] * wsurf[f % NFF] * dA[(size_t)f * L + e];
     double dte = cflFac * vol[e] / iw;  // (CFL * limit * 2) * vol / intWave
     eleDt[e] = dte;
     my = dte;
@@ -77,19 +77,20 @@ __global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__
 }
 
 __global__ void fr_timestep_kernel(double *U, const double *U0, const double *divF, const double *detJ,
-                                   const double *dt, int dtLocal, double coef, int modeB, int NS, int nE,
+                                   const double *dt, int dtLocal, double coef, int modeB, int NS, int nE, int L,
                                    long total) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= total) return;
-  const long pe = i % ((long)NS * nE);
-  const int e = (int)(pe % nE);
+  const long pe = i % ((long)NS * L);
+  const int e = (int)(pe % L);
+  if (e >= nE) return;
   const double dtl = dtLocal ? dt[e] : dt[0];
   if (modeB) U[i] -= coef * divF[i] / detJ[pe] * dtl;
   else U[i] = U0[i] - coef * divF[i] / detJ[pe] * dtl;
 }
 
 __global__ void fr_norm_kernel(const double *divF, const double *detJ, const double *wvol, int NV, int NS, int nE,
-                               int normType, double *partial, unsigned *ticket, double *out) {
+                               int L, int normType, double *partial, unsigned *ticket, double *out) {
   // one thread per element: its per-field norm (spt order as the reference),
   // then per-block totals over elements in index order
   extern __shared__ double sh[];  // [blockDim][NV]
@@ -99,7 +100,7 @@ __global__ void fr_norm_kernel(const double *divF, const double *detJ, const dou
     double r = 0;
     if (e < nE)
       for (int s = 0; s < NS; s++) {
-        double dv = divF[((size_t)v * NS + s) * nE + e], dj = detJ[(size_t)s * nE + e];
+        double dv = divF[((size_t)v * NS + s) * L + e], dj = detJ[(size_t)s * L + e];
         if (normType == 1) r += fabs(dv) * wvol[s];
         else if (normType == 2) r += dv * dv / dj * wvol[s];
         else r = fmax(fabs(dv) / dj, r);
@@ -130,21 +131,23 @@ __global__ void fr_norm_kernel(const double *divF, const double *detJ, const dou
   *ticket = 0;
 }
 
-__global__ void fr_to_device_layout(const double *ref, double *dev, int NV, int NPT, int nE) {
+__global__ void fr_to_device_layout(const double *ref, double *dev, int NV, int NPT, int nE, int L) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // ref index
   const long total = (long)NV * NPT * nE;
   if (i >= total) return;
   const int v = (int)(i % NV);
   const long pe = i / NV;  // pt * nE + e
-  dev[(long)v * NPT * nE + pe] = ref[i];
+  const long pt = pe / nE, e = pe - pt * nE;
+  dev[((long)v * NPT + pt) * L + e] = ref[i];
 }
-__global__ void fr_to_ref_layout(const double *dev, double *ref, int NV, int NPT, int nE) {
+__global__ void fr_to_ref_layout(const double *dev, double *ref, int NV, int NPT, int nE, int L) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // ref index
   const long total = (long)NV * NPT * nE;
   if (i >= total) return;
   const int v = (int)(i % NV);
   const long pe = i / NV;
-  ref[i] = dev[(long)v * NPT * nE + pe];
+  const long pt = pe / nE, e = pe - pt * nE;
+  ref[i] = dev[((long)v * NPT + pt) * L + e];
 }
 template <typename S>
 __global__ void fr_cast_kernel(const double *in, S *out, long n) {
@@ -170,6 +173,7 @@ struct frg_solver {
   Ops1D ops;
   KernelSet ks;
   int nV = 0, nS = 0, nF = 0, nE = 0, nBlk = 0, nRK = 0;
+  int L = 0;  // element stride of device arrays: nE rounded up to a multiple of 32
   size_t sstore = 8;  // bytes of the stored type
   std::vector<double> RKa, RKb;
   cudaStream_t stream = nullptr, ownStream = nullptr;
@@ -260,6 +264,14 @@ frg_status upload_store(frg_solver *s, void **dst, const std::vector<double> &sr
   }
   return FRG_OK;
 }
+// Rows of nE values (element fastest) widened to the padded stride L.
+std::vector<double> pad_rows(const std::vector<double> &src, int nE, int L, double fill) {
+  const size_t rows = src.size() / nE;
+  std::vector<double> out(rows * L, fill);
+  for (size_t r = 0; r < rows; r++) std::memcpy(&out[r * L], &src[r * nE], nE * sizeof(double));
+  return out;
+}
+
 frg_status upload_d(double **dst, const std::vector<double> &src) {
   frg_status st = dalloc(dst, src.size());
   if (st) return st;
@@ -275,7 +287,7 @@ frg_status post_launch(frg_solver *s) {
 
 frg_status ensure_traces(frg_solver *s) {
   if (s->trValid) return FRG_OK;
-  s->ks.trace(s->U, s->tr[s->curTr], s->nE, s->p.vcjhScheme, s->stream);
+  s->ks.trace(s->U, s->tr[s->curTr], s->L, s->nE, s->L, s->p.vcjhScheme, s->stream);
   frg_status st = post_launch(s);
   if (st) return st;
   s->trValid = true;
@@ -284,7 +296,9 @@ frg_status ensure_traces(frg_solver *s) {
 
 StageArgs base_args(frg_solver *s) {
   StageArgs a{};
-  a.nE = s->nE;
+  a.nE = s->L;
+  a.nEle = s->nE;
+  a.ldU = s->L;
   a.nbr = s->nbr;
   a.nrm = s->nrm;
   a.dA = s->dAs;
@@ -321,13 +335,13 @@ const double kCflLimit[6] = {1.393, 0.464, 0.235, 0.1453, 0.100, 0.0736};
 frg_status launch_dt(frg_solver *s) {
   int nb = (s->nE + 255) / 256;
   double fac = s->p.CFL * kCflLimit[s->p.order] * 2;
-  fr_dt_kernel<<<nb, 256, 0, s->stream>>>(s->waveSp, s->dAd, s->vol, s->wsurf, s->nF, s->g.nFF, s->nE, fac,
+  fr_dt_kernel<<<nb, 256, 0, s->stream>>>(s->waveSp, s->dAd, s->vol, s->wsurf, s->nF, s->g.nFF, s->nE, s->L, fac,
                                            s->eleDt, s->blockMin, s->ticket, s->dtDev, s->err);
   return post_launch(s);
 }
 
 frg_status launch_wavesp(frg_solver *s) {
-  s->ks.wavesp(s->tr[s->curTr], s->nrmOwn, s->waveSp, s->nF, s->nE, make_phys(s->p), s->stream);
+  s->ks.wavesp(s->tr[s->curTr], s->nrmOwn, s->waveSp, s->nF, s->L, make_phys(s->p), s->stream);
   return post_launch(s);
 }
 
@@ -422,13 +436,14 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   if (st) return fail(st, "%s", err.c_str());
   s->ops = build_ops1d(p.order, p.vcjhScheme);
   s->nS = s->g.nS; s->nF = s->g.nF; s->nE = s->g.nE;
+  s->L = (s->nE + 31) & ~31;
   if ((st = upload_tables(p.nDims, p.precision))) return st;
   KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType, p.viscous ? 1 : 0};
   if (!select_kernels(key, s->ks, err)) return fail(FRG_ERR_ARG, "%s", err.c_str());
   s->sstore = p.precision == FRG_FP64 ? 8 : 4;
   s->nBlk = (s->nE + s->ks.TE - 1) / s->ks.TE;
   CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-  const size_t nSE = (size_t)s->nV * s->nS * s->nE, nFE = (size_t)s->nV * s->nF * s->nE;
+  const size_t nSE = (size_t)s->nV * s->nS * s->L, nFE = (size_t)s->nV * s->nF * s->L;
   if ((st = dalloc(&s->U, nSE)) || (st = dalloc(&s->U0, nSE)) || (st = dalloc(&s->Acc, nSE))) return st;
   for (int i = 0; i < 2; i++) {
     if ((st = dalloc_bytes(&s->W[i], nSE * s->sstore))) return st;
@@ -439,11 +454,15 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     if ((st = dalloc_bytes(&s->fvn, nFE * s->sstore))) return st;
     if (s->visc2 && (st = dalloc_bytes(&s->fvn2, nFE * s->sstore))) return st;
   }
-  if ((st = upload_store(s.get(), &s->nrm, s->g.nrmC)) || (st = upload_store(s.get(), &s->dAs, s->g.dA)) ||
-      (st = upload_store(s.get(), &s->JG, s->g.JG)) || (st = upload_store(s.get(), &s->detJs, s->g.detJ)))
+  const int nE = s->nE, L = s->L;
+  if ((st = upload_store(s.get(), &s->nrm, pad_rows(s->g.nrmC, nE, L, 0.0))) ||
+      (st = upload_store(s.get(), &s->dAs, pad_rows(s->g.dA, nE, L, 0.0))) ||
+      (st = upload_store(s.get(), &s->JG, pad_rows(s->g.JG, nE, L, 0.0))) ||
+      (st = upload_store(s.get(), &s->detJs, pad_rows(s->g.detJ, nE, L, 1.0))))
     return st;
-  if ((st = upload_d(&s->detJd, s->g.detJ)) || (st = upload_d(&s->nrmOwn, s->g.nrmOwn)) ||
-      (st = upload_d(&s->dAd, s->g.dA)) || (st = upload_d(&s->vol, s->g.vol)))
+  if ((st = upload_d(&s->detJd, pad_rows(s->g.detJ, nE, L, 1.0))) ||
+      (st = upload_d(&s->nrmOwn, pad_rows(s->g.nrmOwn, nE, L, 0.0))) ||
+      (st = upload_d(&s->dAd, pad_rows(s->g.dA, nE, L, 0.0))) || (st = upload_d(&s->vol, pad_rows(s->g.vol, nE, L, 1.0))))
     return st;
   {
     std::vector<double> ws(s->g.nFF), wv(s->nS);
@@ -455,10 +474,24 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     }
     if ((st = upload_d(&s->wsurf, ws)) || (st = upload_d(&s->wvol, wv))) return st;
   }
-  CK(cudaMalloc(&s->nbr, s->g.nbr.size() * sizeof(int)));
-  CK(cudaMemcpy(s->nbr, s->g.nbr.data(), s->g.nbr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  {
+    // neighbour codes with trace indices re-based on the padded stride
+    std::vector<int> nb((size_t)s->nF * L, 0);
+    for (int f = 0; f < s->nF; f++)
+      for (int e = 0; e < nE; e++) {
+        int c = s->g.nbr[(size_t)f * nE + e];
+        if (c >= 0) {
+          long t = c >> 1, fo = t / nE, eo = t - fo * nE, tp = fo * L + eo;
+          if (tp >= (1L << 30)) return fail(FRG_ERR_ARG, "mesh too large for 30-bit trace index");
+          c = (int)((tp << 1) | (c & 1));
+        }
+        nb[(size_t)f * L + e] = c;
+      }
+    CK(cudaMalloc(&s->nbr, nb.size() * sizeof(int)));
+    CK(cudaMemcpy(s->nbr, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   const int nbDt = (s->nE + 255) / 256;
-  if ((st = dalloc(&s->waveSp, (size_t)s->nF * s->nE)) || (st = dalloc(&s->eleDt, (size_t)s->nE)) ||
+  if ((st = dalloc(&s->waveSp, (size_t)s->nF * s->L)) || (st = dalloc(&s->eleDt, (size_t)s->L)) ||
       (st = dalloc(&s->dtDev, 1)) || (st = dalloc(&s->timeDev, 1)) || (st = dalloc(&s->blockMin, (size_t)nbDt)) ||
       (st = dalloc(&s->normPartial, (size_t)nbDt * s->nV)) || (st = dalloc(&s->normOut, (size_t)s->nV)) ||
       (st = dalloc(&s->err, 1)) || (st = dalloc(&s->ticket, 1)))
@@ -559,7 +592,7 @@ frg_status frg_upload(frg_solver *s, int array, const double *host) {
   CK(cudaMemcpyAsync(s->scratchRef, host, n * 8, cudaMemcpyHostToDevice, s->stream));
   fr_to_device_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->scratchRef,
                                                                          array == FRG_U0 ? s->U0 : s->U, s->nV,
-                                                                         s->nS, s->nE);
+                                                                         s->nS, s->nE, s->L);
   if ((st = post_launch(s))) return st;
   if (array == FRG_U_SPTS) s->trValid = false;
   CK(cudaStreamSynchronize(s->stream));
@@ -582,7 +615,7 @@ frg_status frg_download(frg_solver *s, int array, int stage, double *host) {
     case FRG_U_FPTS: {
       if ((st = ensure_traces(s))) return st;
       npt = s->nF;
-      const size_t n = (size_t)s->nV * s->nF * s->nE;
+      const size_t n = (size_t)s->nV * s->nF * s->L;
       if (s->sstore == 8) {
         src = (const double *)s->tr[s->curTr];
       } else {
@@ -593,7 +626,7 @@ frg_status frg_download(frg_solver *s, int array, int stage, double *host) {
         for (int v = 0; v < s->nV; v++)
           for (int q = 0; q < s->nF; q++)
             for (int e = 0; e < s->nE; e++)
-              host[((size_t)q * s->nE + e) * s->nV + v] = f[((size_t)v * s->nF + q) * s->nE + e];
+              host[((size_t)q * s->nE + e) * s->nV + v] = f[((size_t)v * s->nF + q) * s->L + e];
         return FRG_OK;
       }
       break;
@@ -605,11 +638,11 @@ frg_status frg_download(frg_solver *s, int array, int stage, double *host) {
       std::memcpy(host, s->g.detJ.data(), s->g.detJ.size() * 8);
       return FRG_OK;
     case FRG_WAVESP: {
-      std::vector<double> w((size_t)s->nF * s->nE);
+      std::vector<double> w((size_t)s->nF * s->L);
       CK(cudaMemcpyAsync(w.data(), s->waveSp, w.size() * 8, cudaMemcpyDeviceToHost, s->stream));
       CK(cudaStreamSynchronize(s->stream));
       for (int f = 0; f < s->nF; f++)
-        for (int e = 0; e < s->nE; e++) host[(size_t)e * s->nF + f] = w[(size_t)f * s->nE + e];
+        for (int e = 0; e < s->nE; e++) host[(size_t)e * s->nF + f] = w[(size_t)f * s->L + e];
       return FRG_OK;
     }
     case FRG_ELE_DT:
@@ -620,7 +653,7 @@ frg_status frg_download(frg_solver *s, int array, int stage, double *host) {
       return fail(FRG_ERR_ARG, "unknown array %d", array);
   }
   const size_t n = (size_t)s->nV * npt * s->nE;
-  fr_to_ref_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(src, s->scratchRef, s->nV, npt, s->nE);
+  fr_to_ref_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(src, s->scratchRef, s->nV, npt, s->nE, s->L);
   if ((st = post_launch(s))) return st;
   CK(cudaMemcpyAsync(host, s->scratchRef, n * 8, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -658,7 +691,7 @@ extern "C" {
 frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double *divF_dev, void *stream) {
   if (!s || !U_dev || !divF_dev) return fail(FRG_ERR_ARG, "null argument");
   // traces, and for viscous runs the projected viscous fluxes after them
-  const size_t one = (size_t)s->nV * s->nF * s->nE * s->sstore;
+  const size_t one = (size_t)s->nV * s->nF * s->L * s->sstore;
   const size_t oneAligned = (one + 255) & ~size_t(255);
   const size_t need = one + (s->ks.grad ? oneAligned * (s->visc2 ? 2 : 1) : 0);
   if (need > kNoAllocScratchBytes)
@@ -682,9 +715,10 @@ frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double 
   }
   cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
   // traces of the caller's state into the scratch array, then the residual
-  s->ks.trace(U_dev, scratch, s->nE, s->p.vcjhScheme, st);
+  s->ks.trace(U_dev, scratch, s->L, s->nE, s->nE, s->p.vcjhScheme, st);
   CK(cudaGetLastError());
   StageArgs a = base_args(s);
+  a.ldU = s->nE;  // the caller's arrays are dense [nFields][nSpts][nEles]
   a.Uin_d = U_dev;
   a.trIn = scratch;
   a.divF = divF_dev;
@@ -708,7 +742,7 @@ frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double 
 frg_status frg_calc_residual(frg_solver *s, int step) {
   if (!s || step < 0 || step >= s->nRK) return fail(FRG_ERR_ARG, "bad step");
   frg_status st;
-  if (!s->divF[step] && (st = dalloc(&s->divF[step], (size_t)s->nV * s->nS * s->nE))) return st;
+  if (!s->divF[step] && (st = dalloc(&s->divF[step], (size_t)s->nV * s->nS * s->L))) return st;
   // solver::extrapolateU always recomputes the traces of U_spts
   s->trValid = false;
   if ((st = ensure_traces(s))) return st;
@@ -724,32 +758,32 @@ frg_status frg_calc_residual(frg_solver *s, int step) {
 
 frg_status frg_time_step_a(frg_solver *s, int step, double rkval) {
   if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
-  const long n = (long)s->nV * s->nS * s->nE;
+  const long n = (long)s->nV * s->nS * s->L;
   fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
       s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev, s->p.dtType == 2, rkval, 0,
-      s->nS, s->nE, n);
+      s->nS, s->nE, s->L, n);
   s->trValid = false;
   return post_launch(s);
 }
 
 frg_status frg_time_step_b(frg_solver *s, int step) {
   if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
-  const long n = (long)s->nV * s->nS * s->nE;
+  const long n = (long)s->nV * s->nS * s->L;
   fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
       s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev, s->p.dtType == 2,
-      s->RKb[step], 1, s->nS, s->nE, n);
+      s->RKb[step], 1, s->nS, s->nE, s->L, n);
   s->trValid = false;
   return post_launch(s);
 }
 
 frg_status frg_copy_u_to_u0(frg_solver *s) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
-  CK(cudaMemcpyAsync(s->U0, s->U, (size_t)s->nV * s->nS * s->nE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->U0, s->U, (size_t)s->nV * s->nS * s->L * 8, cudaMemcpyDeviceToDevice, s->stream));
   return FRG_OK;
 }
 frg_status frg_copy_u0_to_u(frg_solver *s) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
-  CK(cudaMemcpyAsync(s->U, s->U0, (size_t)s->nV * s->nS * s->nE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->U, s->U0, (size_t)s->nV * s->nS * s->L * 8, cudaMemcpyDeviceToDevice, s->stream));
   s->trValid = false;
   return FRG_OK;
 }
@@ -822,7 +856,7 @@ frg_status frg_residual_norm(frg_solver *s, int normType, double *out) {
   if (!s->divF0Valid) return fail(FRG_ERR_ARG, "no stage-0 residual stored (call frg_calc_residual(0))");
   const int nb = (s->nE + 255) / 256;
   fr_norm_kernel<<<nb, 256, 256 * s->nV * sizeof(double), s->stream>>>(s->divF[0], s->detJd, s->wvol, s->nV, s->nS,
-                                                                        s->nE, normType, s->normPartial, s->ticket,
+                                                                        s->nE, s->L, normType, s->normPartial, s->ticket,
                                                                         s->normOut);
   frg_status st = post_launch(s);
   if (st) return st;
@@ -836,7 +870,7 @@ frg_status frg_set_monitor(frg_solver *s, int enable) {
   if ((enable != 0) == s->monitor) return FRG_OK;
   s->monitor = enable != 0;
   if (s->monitor && !s->divF[0]) {
-    frg_status st = dalloc(&s->divF[0], (size_t)s->nV * s->nS * s->nE);
+    frg_status st = dalloc(&s->divF[0], (size_t)s->nV * s->nS * s->L);
     if (st) return st;
   }
   // the captured steps carry the old flags

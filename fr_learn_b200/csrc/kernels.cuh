@@ -143,7 +143,9 @@ enum : int {
 // Arguments of one stage launch.  Arrays of the stored type S (double, or
 // float in the mixed mode) are passed untyped and cast in the kernel.
 struct StageArgs {
-  int nE;
+  int nE;    // element stride of the mesh arrays (geometry, traces), a multiple of 32
+  int nEle;  // number of real elements
+  int ldU;   // element stride of the state arrays (U, U0, Acc, W, divF)
   const double *Uin_d;  // stage input when stored in double (else null)
   const void *Uin_s;    // stage input in the stored type
   const double *U0;     // state at the start of the step
@@ -239,10 +241,10 @@ __device__ __forceinline__ void load_state(const StageArgs &a, R *Us, int e0) {
   const S *Uin_s = static_cast<const S *>(a.Uin_s);
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= a.nE) continue;
+    if (eg >= a.nEle) continue;
 #pragma unroll
     for (int v = 0; v < NV; v++) {
-      const size_t gi = ((size_t)v * NS + s) * a.nE + eg;
+      const size_t gi = ((size_t)v * NS + s) * a.ldU + eg;
       Us[(v * NS + s) * TE + e] = a.Uin_d ? (R)a.Uin_d[gi] : (R)Uin_s[gi];
     }
   }
@@ -260,7 +262,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
   const bool resid = a.flags & SF_RESIDUAL;
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= nE) continue;
+    if (eg >= a.nEle) continue;
     const int i = s % N1, j = (s / N1) % N1, k = DIM == 3 ? s / (N1 * N1) : 0;
     const int ijk[3] = {i, j, k};
     int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
@@ -285,7 +287,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
         const R g = cs[c] ? op.gR[ca[c]] : -op.gL[ca[c]];
         acc += g * Js[(v * NF + cf[c]) * TE + e];
       }
-      const size_t gi = ((size_t)v * NS + s) * nE + eg;
+      const size_t gi = ((size_t)v * NS + s) * a.ldU + eg;
       const double div = (double)acc;
       if (a.flags & (SF_RESIDUAL | SF_DIVF)) a.divF[gi] = div;
       if (resid) continue;
@@ -322,7 +324,7 @@ __device__ __forceinline__ void trace_phase(const StageArgs &a, const OpTab<R> &
   S *trOut = static_cast<S *>(a.trOut);
   for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= a.nE) continue;
+    if (eg >= a.nEle) continue;
     int dir, side, s0, st;
     fpt_line<C>(f, dir, side, s0, st);
 #pragma unroll
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
   __syncthreads();
   for (int it = tid; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= nE) continue;
+    if (eg >= a.nEle) continue;
     R u[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) u[v] = Us[(v * NS + s) * TE + e];
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
   // ---- B: common flux and jump at flux points
   for (int it = tid; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= nE) continue;
+    if (eg >= a.nEle) continue;
     int dir, side, s0, st;
     fpt_line<C>(f, dir, side, s0, st);
     R own[NV], dis[NV];
@@ -489,7 +491,7 @@ __device__ __forceinline__ void ldg_phase(const StageArgs &a, const OpTab<R> &op
   const S *nrmG = static_cast<const S *>(a.nrm);
   for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= a.nE) continue;
+    if (eg >= a.nEle) continue;
     R own[NV], oth[NV], n[DIM];
     own_trace<C, R, TE>(op, Us, f, e, own);
 #pragma unroll
@@ -519,7 +521,7 @@ __device__ __forceinline__ void gradient_phase(const StageArgs &a, const OpTab<R
   const S *detJG = static_cast<const S *>(a.detJ);
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= a.nE) continue;
+    if (eg >= a.nEle) continue;
     const int i = s % N1, j = (s / N1) % N1, k = DIM == 3 ? s / (N1 * N1) : 0;
     const int ijk[3] = {i, j, k};
     int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
@@ -605,7 +607,7 @@ __global__ void __launch_bounds__(C::NT, 1) fr_visc_grad_kernel(const StageArgs 
   // this side's viscous flux, projected, at every interior flux point
   for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= a.nE || a.nbr[(size_t)f * a.nE + eg] < 0) continue;
+    if (eg >= a.nEle || a.nbr[(size_t)f * a.nE + eg] < 0) continue;
     R u[NV], g[DIM * NV], n[DIM], Fv[DIM][NV];
     own_trace<C, R, TE>(op, Us, f, e, u);
     own_grad_trace<C, R, TE>(op, dUs, f, e, g);
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(C::NT, 1) fr_stage_visc_kernel(const StageArgs
   //  src/solver.cpp:562-596 adds the viscous flux and applies JGinv)
   for (int it = tid; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= nE) continue;
+    if (eg >= a.nEle) continue;
     R u[NV], g[DIM * NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) u[v] = Us[(v * NS + s) * TE + e];
@@ -691,7 +693,7 @@ __global__ void __launch_bounds__(C::NT, 1) fr_stage_visc_kernel(const StageArgs
   // face::calcViscousFlux, src/face.cpp:132-287) and the jumps
   for (int it = tid; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
-    if (eg >= nE) continue;
+    if (eg >= a.nEle) continue;
     int dir, side, s0, st;
     fpt_line<C>(f, dir, side, s0, st);
     R own[NV], dis[NV];
@@ -796,19 +798,21 @@ __global__ void __launch_bounds__(C::NT, 1) fr_stage_visc_kernel(const StageArgs
 // (flux point, element).
 // ----------------------------------------------------------------------------
 template <class C, typename R, typename S>
-__global__ void fr_trace_kernel(const double *__restrict__ U, S *__restrict__ tr, int nE, int vcjh) {
+__global__ void fr_trace_kernel(const double *__restrict__ U, S *__restrict__ tr, int nE, int nEle, int ldU,
+                                int vcjh) {
   constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1;
   const OpTab<R> &op = optab<R>(vcjh, C::P);
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)NF * nE) return;
   const int f = (int)(idx / nE), eg = (int)(idx - (long)f * nE);
+  if (eg >= nEle) return;
   int dir, side, s0, st;
   fpt_line<C>(f, dir, side, s0, st);
 #pragma unroll
   for (int v = 0; v < NV; v++) {
     R t = 0;
 #pragma unroll
-    for (int j = 0; j < N1; j++) t += op.lag[side][j] * (R)U[((size_t)v * NS + s0 + j * st) * nE + eg];
+    for (int j = 0; j < N1; j++) t += op.lag[side][j] * (R)U[((size_t)v * NS + s0 + j * st) * ldU + eg];
     tr[((size_t)v * NF + f) * nE + eg] = (S)t;
   }
 }

@@ -22,9 +22,10 @@ void launch_grad(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_visc_grad_kernel<C, R, S, BC><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
 }
 template <class C, typename R, typename S>
-void launch_trace(const double *U, void *tr, int nE, int vcjh, cudaStream_t st) {
+void launch_trace(const double *U, void *tr, int nE, int nEle, int ldU, int vcjh, cudaStream_t st) {
   long n = (long)C::NF * nE;
-  fr_trace_kernel<C, R, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U, static_cast<S *>(tr), nE, vcjh);
+  fr_trace_kernel<C, R, S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U, static_cast<S *>(tr), nE, nEle, ldU,
+                                                                         vcjh);
 }
 template <int DIM, int NV, typename S>
 void launch_wavesp(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph, cudaStream_t st) {
