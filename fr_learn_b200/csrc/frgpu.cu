@@ -1,6 +1,7 @@
 // frgpu.cu -- the C ABI (include/frgpu.h): handle, device buffers, kernel
 // dispatch over (dimension, order, fields, precision), the RK driver and its
 // CUDA-graph replay.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -15,6 +16,7 @@
 #include "../../include/frgpu.h"
 #include "dispatch.h"
 #include "kernels.cuh"
+#include "kernels_tma.cuh"
 #include "setup.h"
 
 namespace frg {
@@ -193,6 +195,10 @@ struct frg_solver {
   int iter = 0, initIter = 0;
   long long launches = 0;
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [firstIter][curTr]
+  // tensor maps of the TMA stage kernel
+  bool useTma = false;
+  int nBlkTma = 0;
+  CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
 };
 
 namespace {
@@ -319,6 +325,60 @@ StageArgs base_args(frg_solver *s) {
   return a;
 }
 
+// cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
+// libcuda link dependency).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// 2D tensor map over rows x L elements (row stride L), box TE x rows.
+frg_status make_map(CUtensorMap *m, void *base, CUtensorMapDataType dt, int esz, int rows, int L, int TE) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if (rows > 256 || ((size_t)TE * esz) % 16 || ((size_t)L * esz) % 16 || ((uintptr_t)base & 15))
+    return fail(FRG_ERR_ARG, "tensor map shape not TMA-compatible");
+  cuuint64_t dims[2] = {(cuuint64_t)L, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)L * esz};
+  cuuint32_t box[2] = {(cuuint32_t)TE, (cuuint32_t)rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(m, dt, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return FRG_OK;
+}
+
+frg_status setup_tma(frg_solver *s) {
+  const int TE = s->ks.TE_tma, L = s->L, d = s->p.nDims;
+  const CUtensorMapDataType ts = s->sstore == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const int es = (int)s->sstore, nvs = s->nV * s->nS, nvf = s->nV * s->nF;
+  frg_status st;
+  if ((st = make_map(&s->mU, s->U, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, nvs, L, TE)) ||
+      (st = make_map(&s->mAcc, s->Acc, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, nvs, L, TE)) ||
+      (st = make_map(&s->mW[0], s->W[0], ts, es, nvs, L, TE)) || (st = make_map(&s->mW[1], s->W[1], ts, es, nvs, L, TE)) ||
+      (st = make_map(&s->mTr[0], s->tr[0], ts, es, nvf, L, TE)) ||
+      (st = make_map(&s->mTr[1], s->tr[1], ts, es, nvf, L, TE)) ||
+      (st = make_map(&s->mJG, s->JG, ts, es, d * d * s->nS, L, TE)) ||
+      (st = make_map(&s->mDet, s->detJs, ts, es, s->nS, L, TE)) ||
+      (st = make_map(&s->mNrm, s->nrm, ts, es, d * s->nF, L, TE)) ||
+      (st = make_map(&s->mDA, s->dAs, ts, es, s->nF, L, TE)) ||
+      (st = make_map(&s->mNbr, s->nbr, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, s->nF, L, TE)))
+    return st;
+  s->nBlkTma = L / TE;
+  return FRG_OK;
+}
+
 frg_status launch_stage_args(frg_solver *s, StageArgs &a) {
   if (s->ks.grad) {  // viscous: the gradient kernel first (same inputs)
     s->ks.grad(&a, s->nBlk, s->ks.smem, s->stream);
@@ -376,7 +436,24 @@ frg_status enqueue_step(frg_solver *s, bool firstIter, cudaEvent_t *ev = nullptr
       a.flags |= SF_DIVF;
       a.divF = s->divF[0];
     }
-    if ((st = launch_stage_args(s, a))) return st;
+    if (s->useTma) {
+      TmaMaps mm;
+      mm.U = s->mU;
+      mm.Acc = s->mAcc;
+      mm.Win = s->mW[k > 0 ? (k - 1) & 1 : 0];
+      mm.Wout = s->mW[k & 1];
+      mm.trOut = s->mTr[s->curTr ^ 1];
+      mm.JG = s->mJG;
+      mm.det = s->mDet;
+      mm.nrm = s->mNrm;
+      mm.dA = s->mDA;
+      mm.nbr = s->mNbr;
+      s->ks.stage_tma(&a, &mm, s->nBlkTma, s->ks.smem_tma, s->stream);
+      st = post_launch(s);
+    } else {
+      st = launch_stage_args(s, a);
+    }
+    if (st) return st;
     if (ev) CK(cudaEventRecord(ev[2 + k], s->stream));
     s->curTr ^= 1;
   }
@@ -392,6 +469,7 @@ frg_status check_flags(frg_solver *s) {
     if (h & ERRF_NAN) return fail(FRG_ERR_NAN, "NaN encountered in the solution");
     if (h & ERRF_DT) return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
     if (h & ERRF_BC) return fail(FRG_ERR_ARG, "Boundary condition not recognized");
+    if (h & ERRF_TIMEOUT) return fail(FRG_ERR_TIMEOUT, "a bounded device wait gave up");
   }
   return FRG_OK;
 }
@@ -497,6 +575,11 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
       (st = dalloc(&s->err, 1)) || (st = dalloc(&s->ticket, 1)))
     return st;
   if (p.dtType == 0) CK(cudaMemcpy(s->dtDev, &p.dt, sizeof(double), cudaMemcpyHostToDevice));
+  if (s->ks.stage_tma && !s->ks.grad) {
+    const char *env = getenv("FRG_KERNEL");
+    s->useTma = !(env && std::strcmp(env, "generic") == 0);
+    if (s->useTma && (st = setup_tma(s.get()))) return st;
+  }
   CK(cudaDeviceSynchronize());
   *out = s.release();
   return FRG_OK;

@@ -5,6 +5,7 @@
 #pragma once
 #include "dispatch.h"
 #include "kernels.cuh"
+#include "kernels_tma.cuh"
 
 namespace frg {
 namespace {
@@ -12,6 +13,11 @@ namespace {
 template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_stage_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
+}
+template <class C, typename R, typename S, bool BC, int RS>
+void launch_stage_tma(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
+  fr_stage_tma_kernel<C, R, S, BC, RS><<<nBlk, TileT<C, R, S>::NT, smem, st>>>(
+      *static_cast<const StageArgs *>(args), *static_cast<const TmaMaps *>(maps));
 }
 template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage_visc(const void *args, int nBlk, size_t smem, cudaStream_t st) {
@@ -47,6 +53,16 @@ bool make_set(KernelSet &k, std::string &err) {
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if constexpr (C::DIM == 2) {
+    using TT = TileT<C, R, S>;
+    k.stage_tma = &launch_stage_tma<C, R, S, BC, RS>;
+    k.TE_tma = TT::TE;
+    k.smem_tma = TT::SMEM;
+    auto ft = fr_stage_tma_kernel<C, R, S, BC, RS>;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(ft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ft, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  }
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;
 }

@@ -201,3 +201,24 @@ def test_gpu_vs_reference_golden(oracle, name):
         dts.append(s2.dt)
     assert relerr(s2.get("U_spts"), g[pre + "final_U_spts"]) < FP64_TOL
     assert relerr(dts, g[pre + "dt_hist"]) < FP64_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("case", ["periodic", "bump"])
+def test_tma_kernel_matches_generic_kernel(monkeypatch, precision, case):
+    """The TMA-tiled stage kernel of the fused update (2D) and the generic
+    per-thread-load kernel compute the same arithmetic."""
+    from fr_learn_b200 import Solver, box2d, bump2d
+
+    if case == "periodic":
+        mesh, ic, kw = box2d(9, 7, -10, 10, -10, 10, perturb=0.1, seed=21), 1, dict(order=4, riemannType=1, dtType=1)
+    else:
+        mesh, ic, kw = bump2d(12, 5), 0, dict(order=3, riemannType=1, dtType=1, uBound=0.5 * np.sqrt(1.4), pBound=1.0)
+    monkeypatch.setenv("FRG_KERNEL", "generic")
+    a = Solver(mesh, precision=precision, **kw)
+    monkeypatch.delenv("FRG_KERNEL")
+    b = Solver(mesh, precision=precision, **kw)
+    for s in (a, b):
+        s.setInitialCondition(ic)
+        s.update(5)
+    assert relerr(b.get("U_spts"), a.get("U_spts")) < 1e-13
