@@ -22,36 +22,44 @@
 namespace frg {
 
 // ----------------------------------------------------------------- kernels
-__global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__restrict__ dA,
-                             const double *__restrict__ vol, const double *__restrict__ wsurf, int NF, int NFF,
-                             int nE, int L, double cflFac, double *eleDt, double *blockMin, unsigned *ticket,
-                             double *dtOut, unsigned *err) {
+// ele::calcDt (src/ele.cpp:1086-1105) per element, then the global minimum.
+// A block covers 32 elements with 8 warps; warp w sums flux points w, w+8, ...
+// of its lane's element (coalesced: a warp reads 32 consecutive elements of one
+// flux point), the 8 partial sums are added in shared memory, then the minimum
+// is taken with warp shuffles, per-block minima are stored and the last block
+// to finish (threadfence + ticket counter) reduces them.  NaN wins the
+// minimum so it is reported.
+constexpr int kDtSlices = 8;
+__global__ void __launch_bounds__(256) fr_dt_kernel(const double *__restrict__ waveSp, const double *__restrict__ dA,
+                                                    const double *__restrict__ vol, const double *__restrict__ wsurf,
+                                                    int NF, int NFF, int nE, int L, double cflFac, double *eleDt,
+                                                    double *blockMin, unsigned *ticket, double *dtOut,
+                                                    unsigned *err) {
+  __shared__ double part[kDtSlices][32];
   __shared__ double wmin[32];
   __shared__ bool last;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  double my = INFINITY;
-  if (e < nE) {
-    double iw = 0;
-    for (int f = 0; f < NF; f++) iw += waveSp[(size_t)f * L + e] * wsurf[f % NFF] * dA[(size_t)f * L + e];
-    double dte = cflFac * vol[e] / iw;  // (CFL * limit * 2) * vol / intWave
-    eleDt[e] = dte;
-    my = dte;
-  }
-  // NaN must win the minimum so that it is detected
-  for (int o = 16; o > 0; o >>= 1) {
-    double t = __shfl_xor_sync(0xffffffffu, my, o);
-    my = (isnan(t) || t < my) ? t : my;
-  }
-  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = my;
+  const int lane = threadIdx.x & 31, slice = threadIdx.x >> 5;
+  const int e = blockIdx.x * 32 + lane;
+  double sum = 0;
+  if (e < nE)
+    for (int f = slice; f < NF; f += kDtSlices) sum += waveSp[(size_t)f * L + e] * wsurf[f % NFF] * dA[(size_t)f * L + e];
+  part[slice][lane] = sum;
   __syncthreads();
-  if (threadIdx.x < 32) {
-    double v = threadIdx.x < (blockDim.x >> 5) ? wmin[threadIdx.x] : INFINITY;
-    for (int o = 16; o > 0; o >>= 1) {
-      double t = __shfl_xor_sync(0xffffffffu, v, o);
-      v = (isnan(t) || t < v) ? t : v;
+  if (slice == 0) {
+    double my = INFINITY;
+    if (e < nE) {
+      double iw = 0;
+      for (int k = 0; k < kDtSlices; k++) iw += part[k][lane];
+      const double dte = cflFac * vol[e] / iw;  // (CFL * limit * 2) * vol / intWave
+      eleDt[e] = dte;
+      my = dte;
     }
-    if (threadIdx.x == 0) {
-      blockMin[blockIdx.x] = v;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double t = __shfl_xor_sync(0xffffffffu, my, o);
+      my = (isnan(t) || t < my) ? t : my;
+    }
+    if (lane == 0) {
+      blockMin[blockIdx.x] = my;
       __threadfence();
       last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
@@ -60,14 +68,14 @@ __global__ void fr_dt_kernel(const double *__restrict__ waveSp, const double *__
   if (!last) return;
   double v = INFINITY;
   for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-    double t = ((volatile double *)blockMin)[b];
+    const double t = ((volatile double *)blockMin)[b];
     v = (isnan(t) || t < v) ? t : v;
   }
   for (int o = 16; o > 0; o >>= 1) {
-    double t = __shfl_xor_sync(0xffffffffu, v, o);
+    const double t = __shfl_xor_sync(0xffffffffu, v, o);
     v = (isnan(t) || t < v) ? t : v;
   }
-  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = v;
+  if (lane == 0) wmin[slice] = v;
   __syncthreads();
   if (threadIdx.x == 0) {
     double r = INFINITY;
@@ -183,6 +191,7 @@ struct frg_solver {
   double *U = nullptr, *U0 = nullptr, *Acc = nullptr, *divF[5] = {nullptr};
   void *W[2] = {nullptr, nullptr}, *tr[2] = {nullptr, nullptr};
   void *nrm = nullptr, *dAs = nullptr, *JG = nullptr, *detJs = nullptr;
+  void *invDetS = nullptr;  // 1 / detJ in the stored type, for the TMA stage kernel
   void *fvn = nullptr, *fvn2 = nullptr;  // viscous: projected viscous flux per flux point
   bool visc2 = false;                    // 3D with an LDG penalty: second projection needed
   double *detJd = nullptr, *nrmOwn = nullptr, *dAd = nullptr, *vol = nullptr, *wsurf = nullptr, *wvol = nullptr;
@@ -370,7 +379,7 @@ frg_status setup_tma(frg_solver *s) {
       (st = make_map(&s->mTr[0], s->tr[0], ts, es, nvf, L, TE)) ||
       (st = make_map(&s->mTr[1], s->tr[1], ts, es, nvf, L, TE)) ||
       (st = make_map(&s->mJG, s->JG, ts, es, d * d * s->nS, L, TE)) ||
-      (st = make_map(&s->mDet, s->detJs, ts, es, s->nS, L, TE)) ||
+      (st = make_map(&s->mDet, s->invDetS, ts, es, s->nS, L, TE)) ||
       (st = make_map(&s->mNrm, s->nrm, ts, es, d * s->nF, L, TE)) ||
       (st = make_map(&s->mDA, s->dAs, ts, es, s->nF, L, TE)) ||
       (st = make_map(&s->mNbr, s->nbr, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, s->nF, L, TE)))
@@ -393,7 +402,7 @@ frg_status launch_stage_args(frg_solver *s, StageArgs &a) {
 const double kCflLimit[6] = {1.393, 0.464, 0.235, 0.1453, 0.100, 0.0736};
 
 frg_status launch_dt(frg_solver *s) {
-  int nb = (s->nE + 255) / 256;
+  int nb = (s->nE + 31) / 32;
   double fac = s->p.CFL * kCflLimit[s->p.order] * 2;
   fr_dt_kernel<<<nb, 256, 0, s->stream>>>(s->waveSp, s->dAd, s->vol, s->wsurf, s->nF, s->g.nFF, s->nE, s->L, fac,
                                            s->eleDt, s->blockMin, s->ticket, s->dtDev, s->err);
@@ -538,6 +547,11 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
       (st = upload_store(s.get(), &s->JG, pad_rows(s->g.JG, nE, L, 0.0))) ||
       (st = upload_store(s.get(), &s->detJs, pad_rows(s->g.detJ, nE, L, 1.0))))
     return st;
+  {
+    std::vector<double> inv = pad_rows(s->g.detJ, nE, L, 1.0);
+    for (double &x : inv) x = 1.0 / x;
+    if ((st = upload_store(s.get(), &s->invDetS, inv))) return st;
+  }
   if ((st = upload_d(&s->detJd, pad_rows(s->g.detJ, nE, L, 1.0))) ||
       (st = upload_d(&s->nrmOwn, pad_rows(s->g.nrmOwn, nE, L, 0.0))) ||
       (st = upload_d(&s->dAd, pad_rows(s->g.dA, nE, L, 0.0))) || (st = upload_d(&s->vol, pad_rows(s->g.vol, nE, L, 1.0))))
@@ -568,7 +582,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     CK(cudaMalloc(&s->nbr, nb.size() * sizeof(int)));
     CK(cudaMemcpy(s->nbr, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
-  const int nbDt = (s->nE + 255) / 256;
+  const int nbDt = (s->nE + 31) / 32;
   if ((st = dalloc(&s->waveSp, (size_t)s->nF * s->L)) || (st = dalloc(&s->eleDt, (size_t)s->L)) ||
       (st = dalloc(&s->dtDev, 1)) || (st = dalloc(&s->timeDev, 1)) || (st = dalloc(&s->blockMin, (size_t)nbDt)) ||
       (st = dalloc(&s->normPartial, (size_t)nbDt * s->nV)) || (st = dalloc(&s->normOut, (size_t)s->nV)) ||
@@ -630,7 +644,8 @@ frg_status frg_destroy(frg_solver *s) {
                   s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
                   s->blockMin, s->normPartial, s->normOut, s->scratchRef};
   for (double *q : dp) if (q) cudaFree(q);
-  void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->nbr, s->err, s->ticket,
+  void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->invDetS, s->nbr, s->err,
+                s->ticket,
                 s->fvn, s->fvn2};
   for (void *q : vp) if (q) cudaFree(q);
   cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy

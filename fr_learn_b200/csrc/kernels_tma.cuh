@@ -34,7 +34,7 @@ struct TmaMaps {
   CUtensorMap Wout;   // S [NV*NS]: next stage state
   CUtensorMap trOut;  // S [NV*NF]: traces of the new state
   CUtensorMap JG;     // S [DIM*DIM*NS]
-  CUtensorMap det;    // S [NS]
+  CUtensorMap det;    // S [NS]: 1 / detJ
   CUtensorMap nrm;    // S [DIM*NF]
   CUtensorMap dA;     // S [NF]
   CUtensorMap nbr;    // int32 [NF]
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
     const int ijk[3] = {i, j, k};
     int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
     corr_fpts<C>(i, j, k, cf, cs, ca);
-    const double det = (double)sDet[s * TE + e];
+    const double idet = (double)sDet[s * TE + e];  // 1 / detJ
     const double dtl = a.dtLocal ? a.dt[eg] : a.dt[0];
 #pragma unroll
     for (int v = 0; v < NV; v++) {
@@ -303,10 +303,10 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
       if (flags & SF_DIVF) a.divF[((size_t)v * NS + s) * a.ldU + eg] = div;
       double unew;
       if (jam) {
-        unew = sU0[o] - a.aNext * div / det * dtl;
+        unew = sU0[o] - a.aNext * div * idet * dtl;
         if (last) sU0[o] = unew;
       } else {
-        const double t = a.bCur * div / det * dtl;
+        const double t = a.bCur * div * idet * dtl;
         const double base = first ? sU0[o] : sAcc[o];
         if (last) {
           unew = base - t;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
         } else {
           sAcc[o] = base - t;
           const double u0 = first ? base : sU0[o];
-          unew = u0 - a.aNext * div / det * dtl;
+          unew = u0 - a.aNext * div * idet * dtl;
         }
       }
       if (last && (v == 0 || v == NV - 1) && isnan(unew)) atomicOr(a.err, ERRF_NAN);

@@ -42,7 +42,7 @@ __device__ __forceinline__ void inviscid_flux(const R *U, R F[DIM][NV], const Ph
     if constexpr (DIM == 3) F[2][0] = (R)ph.adv[2] * U[0];
   } else if constexpr (DIM == 2) {
     const R g = (R)ph.gamma;
-    R rho = U[0], u = U[1] / rho, v = U[2] / rho, E = U[3];
+    const R rho = U[0], ir = (R)1 / rho, u = U[1] * ir, v = U[2] * ir, E = U[3];
     R p = (g - (R)1.0) * (E - (R)0.5 * rho * (u * u + v * v));
     F[0][0] = rho * u; F[1][0] = rho * v;
     F[0][1] = rho * u * u + p; F[1][1] = rho * u * v;
@@ -50,7 +50,7 @@ __device__ __forceinline__ void inviscid_flux(const R *U, R F[DIM][NV], const Ph
     F[0][3] = (E + p) * u; F[1][3] = (E + p) * v;
   } else {
     const R g = (R)ph.gamma;
-    R rho = U[0], u = U[1] / rho, v = U[2] / rho, w = U[3] / rho, E = U[4];
+    const R rho = U[0], ir = (R)1 / rho, u = U[1] * ir, v = U[2] * ir, w = U[3] * ir, E = U[4];
     R p = (g - (R)1.0) * (E - (R)0.5 * rho * (u * u + v * v + w * w));
     F[0][0] = rho * u; F[1][0] = rho * v; F[2][0] = rho * w;
     F[0][1] = rho * u * u + p; F[1][1] = rho * u * v; F[2][1] = rho * u * w;
@@ -71,26 +71,27 @@ __device__ __forceinline__ R rusanov(const R *UL, const R *UR, const R *n, R *Fn
 #pragma unroll
   for (int i = 0; i < NV; i++) { FnL[i] = 0; FnR[i] = 0; }
   const PR g = (PR)ph.gamma;
-  PR rhoL = UL[0], rhoR = UR[0];
-  PR uL = (PR)UL[1] / rhoL, uR = (PR)UR[1] / rhoR, vL = (PR)UL[2] / rhoL, vR = (PR)UR[2] / rhoR;
+  const PR rhoL = UL[0], rhoR = UR[0], irL = (PR)1 / rhoL, irR = (PR)1 / rhoR;
+  PR uL = (PR)UL[1] * irL, uR = (PR)UR[1] * irR, vL = (PR)UL[2] * irL, vR = (PR)UR[2] * irR;
   PR pL, pR;
   if constexpr (DIM == 2) {
     pL = (g - (PR)1.0) * ((PR)UL[3] - (PR)0.5 * rhoL * (uL * uL + vL * vL));
     pR = (g - (PR)1.0) * ((PR)UR[3] - (PR)0.5 * rhoR * (uR * uR + vR * vR));
   } else {
-    PR wL = (PR)UL[3] / rhoL, wR = (PR)UR[3] / rhoR;
+    PR wL = (PR)UL[3] * irL, wR = (PR)UR[3] * irR;
     pL = (g - (PR)1.0) * ((PR)UL[4] - (PR)0.5 * rhoL * (uL * uL + vL * vL + wL * wL));
     pR = (g - (PR)1.0) * ((PR)UR[4] - (PR)0.5 * rhoR * (uR * uR + vR * vR + wR * wR));
   }
+  const R irLr = (R)irL, irRr = (R)irR;
   R vnL = 0, vnR = 0;
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    vnL += n[d] * UL[d + 1] / UL[0];
-    vnR += n[d] * UR[d + 1] / UR[0];
+    vnL += n[d] * UL[d + 1] * irLr;
+    vnR += n[d] * UR[d + 1] * irRr;
 #pragma unroll
     for (int i = 0; i < NV; i++) { FnL[i] += n[d] * FL[d][i]; FnR[i] += n[d] * FR[d][i]; }
   }
-  R csqL = (R)fmax(g * pL / rhoL, (PR)0.0), csqR = (R)fmax(g * pR / rhoR, (PR)0.0);
+  R csqL = (R)fmax(g * pL * irL, (PR)0.0), csqR = (R)fmax(g * pR * irR, (PR)0.0);
   R eigL = fabs(vnL) + sqrt(csqL), eigR = fabs(vnR) + sqrt(csqR);
   R eig = eigL > eigR ? eigL : eigR;
 #pragma unroll
@@ -103,12 +104,13 @@ template <typename R, typename PR>
 __device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R *Fn, const Phys &ph) {
   const R g = (R)ph.gamma;
   R vL[2], vR[2], um[2], du[4];
-  for (int i = 0; i < 2; i++) { vL[i] = UL[i + 1] / UL[0]; vR[i] = UR[i + 1] / UR[0]; }
+  const R irL = (R)1 / UL[0], irR = (R)1 / UR[0];
+  for (int i = 0; i < 2; i++) { vL[i] = UL[i + 1] * irL; vR[i] = UR[i + 1] * irR; }
   const PR gp = (PR)ph.gamma;
   R pL = (R)((gp - (PR)1.0) * ((PR)UL[3] - ((PR)0.5 * (PR)UL[0] * ((PR)vL[0] * (PR)vL[0] + (PR)vL[1] * (PR)vL[1]))));
   R pR = (R)((gp - (PR)1.0) * ((PR)UR[3] - ((PR)0.5 * (PR)UR[0] * ((PR)vR[0] * (PR)vR[0] + (PR)vR[1] * (PR)vR[1]))));
-  R hL = (UL[3] + pL) / UL[0], hR = (UR[3] + pR) / UR[0];
-  R sq_rho = sqrt(UR[0] / UL[0]);
+  R hL = (UL[3] + pL) * irL, hR = (UR[3] + pR) * irR;
+  R sq_rho = sqrt(UR[0] * irL);
   R rrho = (R)1. / (sq_rho + (R)1.);
   R usq = 0, unm = 0;
   for (int i = 0; i < 2; i++) {
@@ -118,7 +120,7 @@ __device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R *F
   }
   R hm = rrho * (hL + sq_rho * hR);
   R am_sq = (g - (R)1.) * (hm - usq);
-  R am = sqrt(am_sq);
+  R am = sqrt(am_sq), iam = (R)1 / am;
   R rhoUnL = 0, rhoUnR = 0;
   for (int i = 0; i < 2; i++) { rhoUnL += UL[i + 1] * n[i]; rhoUnR += UR[i + 1] * n[i]; }
   Fn[0] = rhoUnL + rhoUnR;
@@ -127,13 +129,15 @@ __device__ __forceinline__ void roe2d(const R *UL, const R *UR, const R *n, R *F
   Fn[3] = rhoUnL * hL + rhoUnR * hR;
   for (int i = 0; i < 4; i++) du[i] = UR[i] - UL[i];
   R lambda0 = fabs(unm), lambdaP = fabs(unm + am), lambdaM = fabs(unm - am);
-  R eps = (R)0.5 * (fabs(rhoUnL / UL[0] - rhoUnR / UR[0]) + fabs(sqrt(g * pL / UL[0]) - sqrt(g * pR / UR[0])));
-  if (lambda0 < (R)2. * eps) lambda0 = (R)0.25 * lambda0 * lambda0 / eps + eps;
-  if (lambdaP < (R)2. * eps) lambdaP = (R)0.25 * lambdaP * lambdaP / eps + eps;
-  if (lambdaM < (R)2. * eps) lambdaM = (R)0.25 * lambdaM * lambdaM / eps + eps;
+  R eps = (R)0.5 * (fabs(rhoUnL * irL - rhoUnR * irR) + fabs(sqrt(g * pL * irL) - sqrt(g * pR * irR)));
+  // the entropy fix is taken only when eps > lambda/2 >= 0, so 1/eps is finite there
+  const R qe = (R)0.25 / eps;
+  if (lambda0 < (R)2. * eps) lambda0 = qe * lambda0 * lambda0 + eps;
+  if (lambdaP < (R)2. * eps) lambdaP = qe * lambdaP * lambdaP + eps;
+  if (lambdaM < (R)2. * eps) lambdaM = qe * lambdaM * lambdaM + eps;
   R a2 = (R)0.5 * (lambdaP + lambdaM) - lambda0;
-  R a3 = (R)0.5 * (lambdaP - lambdaM) / am;
-  R a1 = a2 * (g - (R)1.) / am_sq;
+  R a3 = (R)0.5 * (lambdaP - lambdaM) * iam;
+  R a1 = a2 * (g - (R)1.) * (iam * iam);
   R a4 = a3 * (g - (R)1.);
   R a5 = usq * du[0] - um[0] * du[1] - um[1] * du[2] + du[3];
   R a6 = unm * du[0] - n[0] * du[1] - n[1] * du[2];

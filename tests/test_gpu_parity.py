@@ -207,7 +207,9 @@ def test_gpu_vs_reference_golden(oracle, name):
 @pytest.mark.parametrize("case", ["periodic", "bump"])
 def test_tma_kernel_matches_generic_kernel(monkeypatch, precision, case):
     """The TMA-tiled stage kernel of the fused update (2D) and the generic
-    per-thread-load kernel compute the same arithmetic."""
+    per-thread-load kernel agree: to FP64 rounding in FP64 mode; in mixed mode
+    the TMA kernel multiplies by a stored FP32 1/detJ where the generic kernel
+    divides by detJ, a difference at FP32 rounding level."""
     from fr_learn_b200 import Solver, box2d, bump2d
 
     if case == "periodic":
@@ -221,4 +223,4 @@ def test_tma_kernel_matches_generic_kernel(monkeypatch, precision, case):
     for s in (a, b):
         s.setInitialCondition(ic)
         s.update(5)
-    assert relerr(b.get("U_spts"), a.get("U_spts")) < 1e-13
+    assert relerr(b.get("U_spts"), a.get("U_spts")) < (1e-13 if precision == 0 else 1e-6)
