@@ -26,7 +26,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
 CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu"]
 CXX_SOURCES = ["setup.cpp"]
-HEADERS = ["kernels.cuh", "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
+HEADERS = ["kernels.cuh", "kernels_tma.cuh", "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
 
 
 def _nvcc():

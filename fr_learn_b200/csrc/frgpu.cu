@@ -197,13 +197,20 @@ struct frg_solver {
   double *detJd = nullptr, *nrmOwn = nullptr, *dAd = nullptr, *vol = nullptr, *wsurf = nullptr, *wvol = nullptr;
   int *nbr = nullptr;
   double *waveSp = nullptr, *eleDt = nullptr, *dtDev = nullptr, *timeDev = nullptr, *blockMin = nullptr;
+  int dtCur = 0;  // slot of dtDev[2] holding the current step's dt (two slots
+                  // when the last stage computes the next step's dt)
+  int dtLast = 0;  // slot of the dt the last step used or frg_calc_dt computed
   double *normPartial = nullptr, *normOut = nullptr, *scratchRef = nullptr;
   unsigned *err = nullptr, *ticket = nullptr;
   int curTr = 0;
   bool trValid = false, divF0Valid = false, monitor = false;
   int iter = 0, initIter = 0;
   long long launches = 0;
-  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [firstIter][curTr]
+  // captured steps, [dt mode][trace buffer][dt slot]: dt mode 0 = the previous
+  // step's last stage already computed dt, 1 = dt kernel first, 2 = wave
+  // speeds + dt first
+  cudaGraphExec_t graph[3][2][2] = {};
+  bool dtFresh = false;  // device dt was computed from the current wave speeds
   // tensor maps of the TMA stage kernel
   bool useTma = false;
   int nBlkTma = 0;
@@ -212,6 +219,9 @@ struct frg_solver {
 
 namespace {
 thread_local std::string g_err;
+
+// getCFLLimit (src/global.cpp:45-66)
+const double kCflLimit[6] = {1.393, 0.464, 0.235, 0.1453, 0.100, 0.0736};
 
 frg_status fail(frg_status st, const char *fmt, ...) {
   char buf[512];
@@ -320,7 +330,7 @@ StageArgs base_args(frg_solver *s) {
   a.JG = s->JG;
   a.detJ = s->detJs;
   a.waveSp = s->waveSp;
-  a.dt = s->p.dtType == 2 ? s->eleDt : s->dtDev;
+  a.dt = s->p.dtType == 2 ? s->eleDt : s->dtDev + s->dtCur;
   a.dtLocal = s->p.dtType == 2;
   a.time = s->timeDev;
   a.err = s->err;
@@ -331,6 +341,15 @@ StageArgs base_args(frg_solver *s) {
   a.fvn2Out = s->fvn2;
   a.fvn2In = s->fvn2;
   a.visc2 = s->visc2;
+  a.vol = s->vol;
+  a.dAd = s->dAd;
+  a.wsurf = s->wsurf;
+  a.blockMin = s->blockMin;
+  a.dtNext = s->dtDev + (s->dtCur ^ 1);
+  a.eleDt = s->eleDt;
+  a.ticket = s->ticket;
+  a.cflFac = s->p.CFL * kCflLimit[s->p.order] * 2;
+  a.nff = s->g.nFF;
   return a;
 }
 
@@ -398,14 +417,13 @@ frg_status launch_stage_args(frg_solver *s, StageArgs &a) {
   return post_launch(s);
 }
 
-// getCFLLimit (src/global.cpp:45-66)
-const double kCflLimit[6] = {1.393, 0.464, 0.235, 0.1453, 0.100, 0.0736};
 
 frg_status launch_dt(frg_solver *s) {
   int nb = (s->nE + 31) / 32;
   double fac = s->p.CFL * kCflLimit[s->p.order] * 2;
   fr_dt_kernel<<<nb, 256, 0, s->stream>>>(s->waveSp, s->dAd, s->vol, s->wsurf, s->nF, s->g.nFF, s->nE, s->L, fac,
-                                           s->eleDt, s->blockMin, s->ticket, s->dtDev, s->err);
+                                           s->eleDt, s->blockMin, s->ticket, s->dtDev + s->dtCur, s->err);
+  s->dtLast = s->dtCur;
   return post_launch(s);
 }
 
@@ -414,15 +432,28 @@ frg_status launch_wavesp(frg_solver *s) {
   return post_launch(s);
 }
 
+// The last stage of the TMA kernel computes the next step's global CFL dt.
+bool fused_dt(const frg_solver *s) { return s->useTma && s->p.dtType == 1; }
+
+// dt work at the start of the next fused step (see frg_solver::graph).
+int dt_mode(const frg_solver *s) {
+  if (s->p.dtType == 0) return 0;
+  if (s->iter == s->initIter + 1) return 2;
+  return (fused_dt(s) && s->dtFresh) ? 0 : 1;
+}
+
 // One fused step (the body of solver::update) on the stream.  With `ev`
 // (2 + nRK events) an event is recorded before the dt kernels and after each
-// launch, for frg_time_stages.
-frg_status enqueue_step(frg_solver *s, bool firstIter, cudaEvent_t *ev = nullptr) {
+// launch, for frg_time_stages.  With the TMA kernel the last stage computes
+// the next step's dt (calcDt reads the wave speeds the last stage leaves).
+frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
   frg_status st;
   if (ev) CK(cudaEventRecord(ev[0], s->stream));
   if (s->p.dtType != 0) {
-    if (firstIter && (st = launch_wavesp(s))) return st;
-    if ((st = launch_dt(s))) return st;
+    if (mode == 2 && (st = launch_wavesp(s))) return st;
+    if (mode >= 1 && (st = launch_dt(s))) return st;
+    if (fused_dt(s))  // the slot the last stage will minimise into
+      CK(cudaMemsetAsync(s->dtDev + (s->dtCur ^ 1), 0x7F, sizeof(double), s->stream));
   }
   if (ev) CK(cudaEventRecord(ev[1], s->stream));
   const int nRK = s->nRK;
@@ -445,6 +476,7 @@ frg_status enqueue_step(frg_solver *s, bool firstIter, cudaEvent_t *ev = nullptr
       a.flags |= SF_DIVF;
       a.divF = s->divF[0];
     }
+    if (last && fused_dt(s)) a.flags |= SF_DTNEXT;
     if (s->useTma) {
       TmaMaps mm;
       mm.U = s->mU;
@@ -584,7 +616,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   }
   const int nbDt = (s->nE + 31) / 32;
   if ((st = dalloc(&s->waveSp, (size_t)s->nF * s->L)) || (st = dalloc(&s->eleDt, (size_t)s->L)) ||
-      (st = dalloc(&s->dtDev, 1)) || (st = dalloc(&s->timeDev, 1)) || (st = dalloc(&s->blockMin, (size_t)nbDt)) ||
+      (st = dalloc(&s->dtDev, 2)) || (st = dalloc(&s->timeDev, 1)) || (st = dalloc(&s->blockMin, (size_t)s->L)) ||
       (st = dalloc(&s->normPartial, (size_t)nbDt * s->nV)) || (st = dalloc(&s->normOut, (size_t)s->nV)) ||
       (st = dalloc(&s->err, 1)) || (st = dalloc(&s->ticket, 1)))
     return st;
@@ -638,8 +670,9 @@ frg_status frg_destroy(frg_solver *s) {
   if (!s) return FRG_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (auto &r : s->graph)
-    for (auto &g : r)
-      if (g) cudaGraphExecDestroy(g);
+    for (auto &q : r)
+      for (auto &g : q)
+        if (g) cudaGraphExecDestroy(g);
   double *dp[] = {s->U, s->U0, s->Acc, s->divF[0], s->divF[1], s->divF[2], s->divF[3], s->divF[4], s->detJd,
                   s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
                   s->blockMin, s->normPartial, s->normOut, s->scratchRef};
@@ -849,6 +882,7 @@ frg_status frg_calc_residual(frg_solver *s, int step) {
   a.trIn = s->tr[s->curTr];
   a.divF = s->divF[step];
   a.flags = SF_RESIDUAL | SF_WAVESP;
+  s->dtFresh = false;  // the wave speeds changed
   if ((st = launch_stage_args(s, a))) return st;
   if (step == 0) s->divF0Valid = true;
   return FRG_OK;
@@ -858,7 +892,7 @@ frg_status frg_time_step_a(frg_solver *s, int step, double rkval) {
   if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
   const long n = (long)s->nV * s->nS * s->L;
   fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
-      s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev, s->p.dtType == 2, rkval, 0,
+      s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev + s->dtCur, s->p.dtType == 2, rkval, 0,
       s->nS, s->nE, s->L, n);
   s->trValid = false;
   return post_launch(s);
@@ -868,7 +902,7 @@ frg_status frg_time_step_b(frg_solver *s, int step) {
   if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
   const long n = (long)s->nV * s->nS * s->L;
   fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
-      s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev, s->p.dtType == 2,
+      s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev + s->dtCur, s->p.dtType == 2,
       s->RKb[step], 1, s->nS, s->nE, s->L, n);
   s->trValid = false;
   return post_launch(s);
@@ -898,7 +932,7 @@ frg_status frg_calc_dt(frg_solver *s, double *dt_out) {
   }
   if ((st = check_flags(s))) return st;
   if (dt_out) {
-    CK(cudaMemcpyAsync(dt_out, s->dtDev, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(dt_out, s->dtDev + s->dtCur, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
   }
   return FRG_OK;
@@ -917,14 +951,14 @@ frg_status frg_update(frg_solver *s, int nsteps) {
   if ((st = ensure_traces(s))) return st;
   for (int n = 0; n < nsteps; n++) {
     s->iter++;
-    const int fi = (s->p.dtType != 0 && s->iter == s->initIter + 1) ? 1 : 0;
+    const int mode = dt_mode(s);
     const int ct = s->curTr;
-    cudaGraphExec_t &ge = s->graph[fi][ct];
+    cudaGraphExec_t &ge = s->graph[mode][ct][s->dtCur];
     if (!ge) {
       cudaGraph_t gr;
       long long before = s->launches;
       CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-      st = enqueue_step(s, fi);
+      st = enqueue_step(s, mode);
       cudaError_t ce = cudaStreamEndCapture(s->stream, &gr);
       if (st) return st;
       if (ce != cudaSuccess) return fail(FRG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
@@ -935,8 +969,11 @@ frg_status frg_update(frg_solver *s, int nsteps) {
     }
     CK(cudaGraphLaunch(ge, s->stream));
     // count the kernels the graph holds
-    s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? 1 + fi : 0);
+    s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? mode : 0);
     s->curTr ^= (s->nRK & 1);
+    s->dtFresh = fused_dt(s);
+    s->dtLast = s->dtCur;
+    s->dtCur ^= (int)s->dtFresh;
   }
   if (nsteps > 0) s->divF0Valid = s->monitor;
   return check_flags(s);
@@ -974,15 +1011,16 @@ frg_status frg_set_monitor(frg_solver *s, int enable) {
   // the captured steps carry the old flags
   CK(cudaStreamSynchronize(s->stream));
   for (auto &r : s->graph)
-    for (auto &g : r)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &q : r)
+      for (auto &g : q)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return FRG_OK;
 }
 
 frg_status frg_get_time(const frg_solver *s, double *time, double *dt, int *iter) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
   if (time) { CK(cudaMemcpyAsync(time, s->timeDev, 8, cudaMemcpyDeviceToHost, s->stream)); }
-  if (dt) { CK(cudaMemcpyAsync(dt, s->dtDev, 8, cudaMemcpyDeviceToHost, s->stream)); }
+  if (dt) { CK(cudaMemcpyAsync(dt, s->dtDev + s->dtLast, 8, cudaMemcpyDeviceToHost, s->stream)); }
   CK(cudaStreamSynchronize(s->stream));
   if (iter) *iter = s->iter;
   return FRG_OK;
@@ -990,6 +1028,7 @@ frg_status frg_get_time(const frg_solver *s, double *time, double *dt, int *iter
 
 frg_status frg_set_iter(frg_solver *s, int iter, int initIter) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
+  s->dtFresh = false;
   s->iter = iter;
   s->initIter = initIter;
   return FRG_OK;
@@ -1021,8 +1060,10 @@ frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long
   for (int n = 0; n < nsteps && !st; n++) {
     if (flush) CK(cudaMemsetAsync(flush, n & 0xff, flushBytes, s->stream));
     s->iter++;
-    const bool fi = s->p.dtType != 0 && s->iter == s->initIter + 1;
-    st = enqueue_step(s, fi, ev.data());
+    st = enqueue_step(s, dt_mode(s), ev.data());
+    s->dtFresh = fused_dt(s);
+    s->dtLast = s->dtCur;
+    s->dtCur ^= (int)s->dtFresh;
     if (st) break;
     CK(cudaEventSynchronize(ev[nEv - 1]));
     for (int k = 0; k <= s->nRK; k++) {
@@ -1050,6 +1091,7 @@ namespace {
 // one kernel per reference call.
 frg_status unfused_update(frg_solver *s) {
   frg_status st;
+  s->dtFresh = false;
   s->iter++;
   const int nRK = s->nRK;
   for (int step = 0; step < nRK - 1; step++) {
@@ -1069,7 +1111,7 @@ frg_status unfused_update(frg_solver *s) {
   // time += dt
   double t = 0, dt = 0;
   CK(cudaMemcpyAsync(&t, s->timeDev, 8, cudaMemcpyDeviceToHost, s->stream));
-  CK(cudaMemcpyAsync(&dt, s->dtDev, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(&dt, s->dtDev + s->dtCur, 8, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   t += dt;
   CK(cudaMemcpyAsync(s->timeDev, &t, 8, cudaMemcpyHostToDevice, s->stream));

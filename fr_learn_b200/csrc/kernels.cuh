@@ -137,7 +137,8 @@ enum : int {
   SF_RESIDUAL = 8,  // solver::calcResidual only: write divF, no update
   SF_JAMESON = 16,  // timeType 5: every stage U = U0 - a t
   SF_TIME = 32,     // advance the device time by dt (block 0)
-  SF_DIVF = 64      // also store divF (residual monitoring) during an update
+  SF_DIVF = 64,     // also store divF (residual monitoring) during an update
+  SF_DTNEXT = 128   // last stage: compute the next step's CFL dt (TMA kernel)
 };
 
 // Arguments of one stage launch.  Arrays of the stored type S (double, or
@@ -171,6 +172,12 @@ struct StageArgs {
   void *fvnOut, *fvn2Out;
   const void *fvnIn, *fvn2In;
   int visc2;
+  // SF_DTNEXT: the next step's dt (ele::calcDt + the global minimum)
+  const double *vol, *dAd, *wsurf;
+  double *blockMin, *dtNext, *eleDt;
+  unsigned *ticket;
+  double cflFac;
+  int nff;
   Phys ph;
 };
 

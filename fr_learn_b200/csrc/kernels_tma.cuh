@@ -97,7 +97,7 @@ struct TileT {
     (void)te;
     return NV * NS * 8 * 2 + NV * NS * (int)sizeof(R) + D * D * NS * (int)sizeof(S) + NS * (int)sizeof(S) +
            D * NF * (int)sizeof(S) + NF * (int)sizeof(S) + NF * 4 + D * NV * NS * (int)sizeof(R) +
-           NV * NF * (int)sizeof(R);
+           NV * NF * (int)sizeof(R) + NF * 8;
   }
   static constexpr int PER_ELE = per_ele(0);
   static constexpr int TE = (16 * PER_ELE <= 72 * 1024) ? 16 : (8 * PER_ELE <= 72 * 1024) ? 8 : 4;
@@ -114,7 +114,8 @@ struct TileT {
   static constexpr int oNbr = oDA + al(NF * TE * (int)sizeof(S));
   static constexpr int oFs = oNbr + al(NF * TE * 4);
   static constexpr int oJs = oFs + al(D * NV * NS * TE * (int)sizeof(R));
-  static constexpr int oBar = oJs + al(NV * NF * TE * (int)sizeof(R));
+  static constexpr int oWs = oJs + al(NV * NF * TE * (int)sizeof(R));
+  static constexpr int oBar = oWs + al(NF * TE * 8);
   static constexpr int SMEM = oBar + 64 + 128;  // + room to align the base
 };
 
@@ -137,6 +138,7 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
   int *sNbr = reinterpret_cast<int *>(smem_raw + T::oNbr);
   R *Fs = reinterpret_cast<R *>(smem_raw + T::oFs);
   R *Js = reinterpret_cast<R *>(smem_raw + T::oJs);
+  double *sWs = reinterpret_cast<double *>(smem_raw + T::oWs);
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::oBar);
 #undef smem_raw
 
@@ -263,7 +265,10 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
     const R *UR = right ? own : oth;
     R Fn[NV];
     const R ws = inviscid_common<C, R, BC, RS>(UL, UR, n, code, Fn, ph);
-    if ((flags & SF_WAVESP) && !right && ws >= 0) a.waveSp[(size_t)f * L + eg] = (double)ws;
+    const bool upd = !right && ws >= 0;
+    if ((flags & SF_WAVESP) && upd) a.waveSp[(size_t)f * L + eg] = (double)ws;
+    if (flags & SF_DTNEXT)  // this flux point's term of ele::calcDt's surface integral
+      sWs[f * TE + e] = (upd ? (double)ws : a.waveSp[(size_t)f * L + eg]) * a.wsurf[f % a.nff] * a.dAd[(size_t)f * L + eg];
 #pragma unroll
     for (int v = 0; v < NV; v++) {
       const R fo = right ? -Fn[v] * dA : Fn[v] * dA;
@@ -351,8 +356,35 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
   if (tid == 0) {
     tma_store2d(&m.trOut, e0, 0, Js);
     tma_commit();
-    tma_wait_reads();
   }
+  if (flags & SF_DTNEXT) {
+    // ele::calcDt for this block's elements with the wave speeds this stage
+    // left (src/ele.cpp:1086-1105; flux points summed in order), then the
+    // global minimum by a 64-bit atomicMin on the bit pattern (positive
+    // doubles order like their bit patterns) into the next step's dt slot,
+    // which the host set to a huge value before the step.
+    if (tid < 32) {
+      double my = INFINITY;
+      const int eg = e0 + tid;
+      if (tid < TE && eg < a.nEle) {
+        double iw = 0;
+#pragma unroll
+        for (int f = 0; f < NF; f++) iw += sWs[f * TE + tid];
+        const double dte = a.cflFac * a.vol[eg] / iw;
+        a.eleDt[eg] = dte;
+        my = dte;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, my, o);
+        my = (isnan(t) || t < my) ? t : my;
+      }
+      if (tid == 0) {
+        if (!(my > 1e-13)) atomicOr(a.err, ERRF_DT);  // also catches NaN
+        else atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext), (unsigned long long)__double_as_longlong(my));
+      }
+    }
+  }
+  if (tid == 0) tma_wait_reads();
   return;
 
 timeout:
