@@ -21,11 +21,17 @@ struct KernelSet {
   void (*trace)(const double *U, void *tr, int nE, int nEle, int ldU, int vcjh, cudaStream_t st) = nullptr;
   void (*wavesp)(const void *tr, const double *nrmOwn, double *ws, int NF, int nE, const Phys &ph,
                  cudaStream_t st) = nullptr;
-  // the fused-update stage kernel with TMA tile movement (2D inviscid);
-  // `maps` points at a TmaMaps
-  void (*stage_tma)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
-  int TE_tma = 0;
-  size_t smem_tma = 0;
+  // the fused-update stage kernel with TMA tile movement (2D inviscid), in
+  // several tile shapes (elements x threads per block) for the autotuner;
+  // `maps` points at a TmaMaps built for that variant's tile width
+  struct TmaVariant {
+    void (*launch)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
+    int TE = 0, NT = 0;
+    size_t smem = 0;
+  };
+  static constexpr int kMaxTma = 4;
+  TmaVariant tma[kMaxTma];
+  int nTma = 0;
   int TE = 0;       // elements per block
   int NT = 0;       // threads per block
   size_t smem = 0;  // dynamic shared memory per block

@@ -213,6 +213,7 @@ struct frg_solver {
   bool dtFresh = false;  // device dt was computed from the current wave speeds
   // tensor maps of the TMA stage kernel
   bool useTma = false;
+  int tmaVar = 0;  // tile-shape variant of the TMA kernel (frg_autotune)
   int nBlkTma = 0;
   CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
 };
@@ -388,7 +389,7 @@ frg_status make_map(CUtensorMap *m, void *base, CUtensorMapDataType dt, int esz,
 }
 
 frg_status setup_tma(frg_solver *s) {
-  const int TE = s->ks.TE_tma, L = s->L, d = s->p.nDims;
+  const int TE = s->ks.tma[s->tmaVar].TE, L = s->L, d = s->p.nDims;
   const CUtensorMapDataType ts = s->sstore == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   const int es = (int)s->sstore, nvs = s->nV * s->nS, nvf = s->nV * s->nF;
   frg_status st;
@@ -430,6 +431,13 @@ frg_status launch_dt(frg_solver *s) {
 frg_status launch_wavesp(frg_solver *s) {
   s->ks.wavesp(s->tr[s->curTr], s->nrmOwn, s->waveSp, s->nF, s->L, make_phys(s->p), s->stream);
   return post_launch(s);
+}
+
+void drop_graphs(frg_solver *s) {
+  for (auto &r : s->graph)
+    for (auto &q : r)
+      for (auto &g : q)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 // The last stage of the TMA kernel computes the next step's global CFL dt.
@@ -489,7 +497,8 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       mm.nrm = s->mNrm;
       mm.dA = s->mDA;
       mm.nbr = s->mNbr;
-      s->ks.stage_tma(&a, &mm, s->nBlkTma, s->ks.smem_tma, s->stream);
+      const KernelSet::TmaVariant &tv = s->ks.tma[s->tmaVar];
+      tv.launch(&a, &mm, s->nBlkTma, tv.smem, s->stream);
       st = post_launch(s);
     } else {
       st = launch_stage_args(s, a);
@@ -621,7 +630,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
       (st = dalloc(&s->err, 1)) || (st = dalloc(&s->ticket, 1)))
     return st;
   if (p.dtType == 0) CK(cudaMemcpy(s->dtDev, &p.dt, sizeof(double), cudaMemcpyHostToDevice));
-  if (s->ks.stage_tma && !s->ks.grad) {
+  if (s->ks.nTma > 0 && !s->ks.grad) {
     const char *env = getenv("FRG_KERNEL");
     s->useTma = !(env && std::strcmp(env, "generic") == 0);
     if (s->useTma && (st = setup_tma(s.get()))) return st;
@@ -669,10 +678,7 @@ frg_status frg_inspect_geometry(const frg_params *params, const frg_mesh *mesh, 
 frg_status frg_destroy(frg_solver *s) {
   if (!s) return FRG_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
-  for (auto &r : s->graph)
-    for (auto &q : r)
-      for (auto &g : q)
-        if (g) cudaGraphExecDestroy(g);
+  drop_graphs(s);
   double *dp[] = {s->U, s->U0, s->Acc, s->divF[0], s->divF[1], s->divF[2], s->divF[3], s->divF[4], s->detJd,
                   s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
                   s->blockMin, s->normPartial, s->normOut, s->scratchRef};
@@ -1010,10 +1016,7 @@ frg_status frg_set_monitor(frg_solver *s, int enable) {
   }
   // the captured steps carry the old flags
   CK(cudaStreamSynchronize(s->stream));
-  for (auto &r : s->graph)
-    for (auto &q : r)
-      for (auto &g : q)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(s);
   return FRG_OK;
 }
 
@@ -1045,6 +1048,94 @@ frg_status frg_set_stream(frg_solver *s, void *stream) {
   CK(cudaStreamSynchronize(s->stream));
   if (!s->ownStream) s->ownStream = s->stream;
   s->stream = stream ? (cudaStream_t)stream : s->ownStream;
+  return FRG_OK;
+}
+
+frg_status frg_set_tile_variant(frg_solver *s, int variant) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  if (!s->useTma) return variant == 0 ? FRG_OK : fail(FRG_ERR_ARG, "no TMA kernel in use");
+  if (variant < 0 || variant >= s->ks.nTma) return fail(FRG_ERR_ARG, "tile variant out of range");
+  CK(cudaStreamSynchronize(s->stream));
+  drop_graphs(s);
+  s->tmaVar = variant;
+  return setup_tma(s);
+}
+
+frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out) {
+  if (!s || nsteps < 1) return fail(FRG_ERR_ARG, "bad arguments");
+  const int nVar = s->useTma ? s->ks.nTma : 1;
+  if (nVar > 1 && !(s->p.timeType == 0 && s->p.dtType != 0)) {
+    // the trial steps advance the solution: keep everything they change
+    const size_t nU = (size_t)s->nV * s->nS * s->L, nW = (size_t)s->nF * s->L, nD = (size_t)s->L;
+    double *save = nullptr;
+    frg_status st = dalloc(&save, 2 * nU + nW + nD + 3);
+    if (st) return st;
+    double *sU = save, *sD0 = save + nU, *sWs = save + 2 * nU, *sEd = sWs + nW, *sDt = sEd + nD;
+    const bool hadDiv = s->divF0Valid && s->divF[0];
+    auto cp = [&](double *dst, const double *src, size_t n) {
+      return cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, s->stream);
+    };
+    CK(cp(sU, s->U, nU));
+    if (hadDiv) CK(cp(sD0, s->divF[0], nU));
+    CK(cp(sWs, s->waveSp, nW));
+    CK(cp(sEd, s->eleDt, nD));
+    CK(cp(sDt, s->dtDev, 2));
+    CK(cp(sDt + 2, s->timeDev, 1));
+    const int iter = s->iter, dtCur = s->dtCur, dtLast = s->dtLast, curTr = s->curTr;
+    const bool dtFresh = s->dtFresh, divValid = s->divF0Valid;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    // three interleaved rounds, the best of each candidate counts, so that a
+    // clock ramp or a neighbour's burst does not decide
+    double msv[KernelSet::kMaxTma];
+    for (int v = 0; v < nVar; v++) msv[v] = 1e300;
+    for (int round = 0; round < 3 && !st; round++)
+      for (int v = 0; v < nVar && !st; v++) {
+        CK(cudaStreamSynchronize(s->stream));
+        drop_graphs(s);
+        s->tmaVar = v;
+        if ((st = setup_tma(s)) || (st = frg_update(s, 1))) break;
+        CK(cudaEventRecord(e0, s->stream));
+        if ((st = frg_update(s, nsteps))) break;
+        CK(cudaEventRecord(e1, s->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        msv[v] = std::min(msv[v], (double)ms / nsteps);
+      }
+    int best = 0;
+    for (int v = 0; v < nVar; v++) {
+      if (ms_out) ms_out[v] = msv[v];
+      if (msv[v] < msv[best]) best = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaStreamSynchronize(s->stream));
+    drop_graphs(s);
+    s->tmaVar = best;
+    frg_status st2 = setup_tma(s);
+    CK(cp(s->U, sU, nU));
+    if (hadDiv) CK(cp(s->divF[0], sD0, nU));
+    CK(cp(s->waveSp, sWs, nW));
+    CK(cp(s->eleDt, sEd, nD));
+    CK(cp(s->dtDev, sDt, 2));
+    CK(cp(s->timeDev, sDt + 2, 1));
+    CK(cudaStreamSynchronize(s->stream));
+    cudaFree(save);
+    s->iter = iter;
+    s->dtCur = dtCur;
+    s->dtLast = dtLast;
+    s->curTr = curTr;
+    s->dtFresh = dtFresh;
+    s->trValid = false;  // the trace buffers hold the trial steps' traces
+    s->divF0Valid = divValid;
+    if (st) return st;
+    if (st2) return st2;
+  } else if (ms_out) {
+    ms_out[0] = 0;
+  }
+  if (variant_out) *variant_out = s->tmaVar;
   return FRG_OK;
 }
 

@@ -267,6 +267,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
   S *Wout = static_cast<S *>(a.Wout);
   const int nE = a.nE;
   const bool resid = a.flags & SF_RESIDUAL;
+  const double dtG = (resid || a.dtLocal) ? 0.0 : __ldg(a.dt);
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
     if (eg >= a.nEle) continue;
@@ -277,7 +278,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
     double det = 0, dtl = 0;
     if (!resid) {
       det = (double)detJG[(size_t)s * nE + eg];
-      dtl = a.dtLocal ? a.dt[eg] : a.dt[0];
+      dtl = a.dtLocal ? a.dt[eg] : dtG;
     }
 #pragma unroll
     for (int v = 0; v < NV; v++) {

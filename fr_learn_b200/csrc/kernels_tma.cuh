@@ -89,8 +89,9 @@ __device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Tile of the TMA kernel: TE elements (box inner extent TE * sizeof >= 16 B),
-// NT threads; shared memory ~64 KB or less so three blocks share an SM.
-template <class C, typename R, typename S>
+// NT threads.  TE_ = 0 picks the widest of 16/8/4 elements whose shared
+// memory stays within 72 KB (three blocks per SM); TE_ = -1 half of that.
+template <class C, typename R, typename S, int TE_ = 0, int NT_ = 128>
 struct TileT {
   static constexpr int NS = C::NS, NF = C::NF, NV = C::NV, D = C::DIM;
   static constexpr int per_ele(int te) {
@@ -100,8 +101,11 @@ struct TileT {
            NV * NF * (int)sizeof(R) + NF * 8;
   }
   static constexpr int PER_ELE = per_ele(0);
-  static constexpr int TE = (16 * PER_ELE <= 72 * 1024) ? 16 : (8 * PER_ELE <= 72 * 1024) ? 8 : 4;
-  static constexpr int NT = 128;
+  static constexpr int TE_AUTO = (16 * PER_ELE <= 72 * 1024) ? 16 : (8 * PER_ELE <= 72 * 1024) ? 8 : 4;
+  static constexpr int TE = TE_ > 0 ? TE_ : TE_ == 0 ? TE_AUTO : (TE_AUTO > 4 ? TE_AUTO / 2 : 4);
+  static constexpr int NT = NT_;
+  // blocks per SM the register budget is sized for
+  static constexpr int MINB = NT_ >= 256 ? 2 : NT_ >= 192 ? 2 : 1;
   static constexpr int al(int b) { return (b + 127) & ~127; }
   // byte offsets of the shared-memory regions (each 128-byte aligned)
   static constexpr int oU0 = 0;
@@ -119,10 +123,11 @@ struct TileT {
   static constexpr int SMEM = oBar + 64 + 128;  // + room to align the base
 };
 
-template <class C, typename R, typename S, bool BC, int RS>
-__global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a, const __grid_constant__ TmaMaps m) {
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
+__global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
+    fr_stage_tma_kernel(const StageArgs a, const __grid_constant__ TmaMaps m) {
   static_assert(sizeof(R) == sizeof(S), "stage state is loaded straight into the compute buffer");
-  using T = TileT<C, R, S>;
+  using T = TileT<C, R, S, TEV, NTV>;
   constexpr int TE = T::TE, NT = T::NT, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // bulk-tensor destinations start on 128-byte boundaries
@@ -173,6 +178,9 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
     if (needU0) tma_load2d(sU0, &m.U, e0, 0, &bar[2]);
     if (needAcc) tma_load2d(sAcc, &m.Acc, e0, 0, &bar[2]);
   }
+
+  // the global dt, fetched while the tiles are in flight
+  const double dtG = a.dtLocal ? 0.0 : __ldg(a.dt);
 
   // ---- group 0: gathers of neighbour traces, then phase A
   bool ok = mbar_wait(&bar[0], 0);
@@ -287,7 +295,7 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
     int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
     corr_fpts<C>(i, j, k, cf, cs, ca);
     const double idet = (double)sDet[s * TE + e];  // 1 / detJ
-    const double dtl = a.dtLocal ? a.dt[eg] : a.dt[0];
+    const double dtl = a.dtLocal ? a.dt[eg] : dtG;
 #pragma unroll
     for (int v = 0; v < NV; v++) {
       R acc = 0;
@@ -326,7 +334,7 @@ __global__ void __launch_bounds__(128, 1) fr_stage_tma_kernel(const StageArgs a,
       Us[o] = (R)(last ? unew : (double)(S)unew);
     }
   }
-  if ((flags & SF_TIME) && blockIdx.x == 0 && tid == 0) *a.time += a.dt[0];
+  if ((flags & SF_TIME) && blockIdx.x == 0 && tid == 0) *a.time += dtG;
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {

@@ -14,10 +14,24 @@ template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_stage_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
 }
-template <class C, typename R, typename S, bool BC, int RS>
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 void launch_stage_tma(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
-  fr_stage_tma_kernel<C, R, S, BC, RS><<<nBlk, TileT<C, R, S>::NT, smem, st>>>(
-      *static_cast<const StageArgs *>(args), *static_cast<const TmaMaps *>(maps));
+  fr_stage_tma_kernel<C, R, S, BC, RS, TEV, NTV><<<nBlk, NTV, smem, st>>>(*static_cast<const StageArgs *>(args),
+                                                                          *static_cast<const TmaMaps *>(maps));
+}
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
+cudaError_t add_tma_variant(KernelSet &k) {
+  using TT = TileT<C, R, S, TEV, NTV>;
+  KernelSet::TmaVariant &v = k.tma[k.nTma++];
+  v.launch = &launch_stage_tma<C, R, S, BC, RS, TEV, NTV>;
+  v.TE = TT::TE;
+  v.NT = NTV;
+  v.smem = TT::SMEM;
+  auto ft = fr_stage_tma_kernel<C, R, S, BC, RS, TEV, NTV>;
+  cudaError_t e = cudaFuncSetAttribute(ft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ft, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  return e;
 }
 template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage_visc(const void *args, int nBlk, size_t smem, cudaStream_t st) {
@@ -54,14 +68,12 @@ bool make_set(KernelSet &k, std::string &err) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if constexpr (C::DIM == 2) {
-    using TT = TileT<C, R, S>;
-    k.stage_tma = &launch_stage_tma<C, R, S, BC, RS>;
-    k.TE_tma = TT::TE;
-    k.smem_tma = TT::SMEM;
-    auto ft = fr_stage_tma_kernel<C, R, S, BC, RS>;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(ft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::SMEM);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(ft, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    // variant 0 is the default; the others are candidates for frg_autotune
+    k.nTma = 0;
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, 0, 128>(k);
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, 0, 256>(k);
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, 0, 192>(k);
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -1, 128>(k);
   }
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;

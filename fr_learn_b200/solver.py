@@ -99,6 +99,8 @@ def lib():
         "frg_set_stream": ([vp, vp], i),
         "frg_calc_residual_noalloc": ([vp, vp, vp, vp], i),
         "frg_time_stages": ([vp, i, vp, C.c_ulonglong, vp], i),
+        "frg_autotune": ([vp, i, C.POINTER(C.c_int), vp], i),
+        "frg_set_tile_variant": ([vp, i], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -253,6 +255,19 @@ class Solver:
         """Run on a caller's cudaStream_t (an int handle, e.g. torch's
         ``stream.cuda_stream``); None restores the solver's own stream."""
         _check(lib().frg_set_stream(self.h, stream_ptr))
+
+    def autotune(self, nsteps=5):
+        """Pick the fastest tile shape of the fused stage kernel by timing
+        `nsteps` steps of each candidate; the solution is left unchanged.
+        Returns (chosen index, per-candidate ms per step)."""
+        v = C.c_int()
+        out = np.zeros(4)
+        _check(lib().frg_autotune(self.h, nsteps, C.byref(v), out.ctypes.data))
+        return v.value, out
+
+    def set_tile_variant(self, v):
+        """Select a tile shape of the fused stage kernel by index."""
+        _check(lib().frg_set_tile_variant(self.h, v))
 
     def time_stages(self, nsteps, flush_ptr=None, flush_bytes=0):
         """Mean per-launch device time (ms) of [dt kernels, stage 0..nRK-1]."""

@@ -197,6 +197,16 @@ frg_status frg_set_stream(frg_solver *s, void *stream);
  * of the per-step dt / wave-speed kernels, ms_out[1 + k] = mean time of RK
  * stage k's kernel, all in milliseconds ([1 + nRK] entries). */
 frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long long flushBytes, double *ms_out);
+/* Picks the fastest tile shape (elements x threads per block) of the fused
+ * TMA stage kernel for this mesh and configuration by timing `nsteps` steps
+ * of each candidate, then restores the solution, time, dt and iteration the
+ * handle had.  Results do not depend on the choice.  `variant_out` receives
+ * the chosen index; `ms_out` (may be NULL) one time per step per candidate
+ * (up to 4 entries).  A no-op where the TMA kernel is not used.  No
+ * counterpart in the reference, which has a single CPU code path. */
+frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out);
+/* Selects a tile shape of the TMA stage kernel by index (0 = default). */
+frg_status frg_set_tile_variant(frg_solver *s, int variant);
 /* Device-side launch counter: kernels launched by this handle so far. */
 frg_status frg_launch_count(const frg_solver *s, long long *count);
 

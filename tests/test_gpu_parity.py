@@ -224,3 +224,38 @@ def test_tma_kernel_matches_generic_kernel(monkeypatch, precision, case):
         s.setInitialCondition(ic)
         s.update(5)
     assert relerr(b.get("U_spts"), a.get("U_spts")) < (1e-13 if precision == 0 else 1e-6)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("case", ["periodic", "bump"])
+def test_tile_variants_identical_and_autotune_restores(precision, case):
+    """Every tile shape of the TMA stage kernel gives bit-identical results
+    (the per-element arithmetic does not depend on the tile), and autotune
+    leaves the solution, time and dt where they were."""
+    from fr_learn_b200 import Solver, box2d, bump2d
+
+    if case == "periodic":
+        mesh, ic, kw = box2d(9, 7, -10, 10, -10, 10, perturb=0.1, seed=21), 1, dict(order=4, riemannType=1, dtType=1)
+    else:
+        mesh, ic, kw = bump2d(12, 5), 0, dict(order=3, riemannType=1, dtType=1, uBound=0.5 * np.sqrt(1.4), pBound=1.0)
+    ref = None
+    for v in range(4):
+        s = Solver(mesh, precision=precision, **kw)
+        s.set_tile_variant(v)
+        s.setInitialCondition(ic)
+        s.update(4)
+        U = s.get("U_spts")
+        if ref is None:
+            ref = (U, s.time, s.dt)
+        else:
+            assert np.array_equal(U, ref[0]), f"variant {v}"
+            assert s.time == ref[1] and s.dt == ref[2]
+    s = Solver(mesh, precision=precision, **kw)
+    s.setInitialCondition(ic)
+    s.update(2)
+    U2, t2, dt2 = s.get("U_spts"), s.time, s.dt
+    v, ms = s.autotune(3)
+    assert 0 <= v < 4 and ms[v] > 0
+    assert np.array_equal(s.get("U_spts"), U2) and s.time == t2 and s.dt == dt2
+    s.update(2)
+    assert np.array_equal(s.get("U_spts"), ref[0])
