@@ -24,9 +24,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC"] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
-CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu"]
+CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu",
+              "adjoint_2d.cu", "adjoint_3d.cu"]
 CXX_SOURCES = ["setup.cpp"]
-HEADERS = ["kernels.cuh", "kernels_tma.cuh", "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
+HEADERS = ["kernels.cuh", "kernels_tma.cuh", "adjoint.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
+           "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
 
 
 def _nvcc():

@@ -41,6 +41,24 @@ struct KernelKey {
   int nDims, P, NV, precision, bc, riemann, viscous;
 };
 
+struct AdjArgs;
+// The discrete-adjoint kernels of one configuration (FP64 only).
+struct AdjSet {
+  void (*face)(const AdjArgs &a, cudaStream_t st) = nullptr;
+  void (*elem)(const AdjArgs &a, cudaStream_t st) = nullptr;
+  // objectives: per-block partial sums into `part` (obj_blocks entries)
+  void (*entropy)(const double *U, const double *detJ, const double *wvol, int nE, int L, const Phys &ph,
+                  double *grad, double *part, cudaStream_t st) = nullptr;
+  void (*wallp)(const double *U, const int *nbr, const double *dA, const double *wsurf, int vcjh, int nE, int L,
+                int bcWall, const Phys &ph, double *grad, double *part, cudaStream_t st) = nullptr;
+  int entropyBlocks = 0;  // partial sums written by `entropy` (grid size)
+  int TE = 0;             // elements per block of `elem`
+};
+bool select_adj_2d(const KernelKey &key, AdjSet &k, std::string &err);
+bool select_adj_3d(const KernelKey &key, AdjSet &k, std::string &err);
+cudaError_t upload_tables_adj_2d();
+cudaError_t upload_tables_adj_3d();
+
 // Fills `k` for the key, or returns false with `err` set.
 bool select_2d_f64(const KernelKey &key, KernelSet &k, std::string &err);
 bool select_2d_f32(const KernelKey &key, KernelSet &k, std::string &err);

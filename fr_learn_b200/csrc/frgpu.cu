@@ -17,6 +17,7 @@
 #include "dispatch.h"
 #include "kernels.cuh"
 #include "kernels_tma.cuh"
+#include "adjoint.cuh"
 #include "setup.h"
 
 namespace frg {
@@ -176,6 +177,9 @@ bool select_kernels(const KernelKey &key, KernelSet &k, std::string &err) {
 
 using namespace frg;
 
+struct AdjState;  // discrete-adjoint buffers (end of this file)
+void adj_free(frg_solver *s);
+
 // -------------------------------------------------------------- the handle
 struct frg_solver {
   frg_params p{};
@@ -216,6 +220,7 @@ struct frg_solver {
   int tmaVar = 0;  // tile-shape variant of the TMA kernel (frg_autotune)
   int nBlkTma = 0;
   CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
+  AdjState *adj = nullptr;
 };
 
 namespace {
@@ -678,6 +683,7 @@ frg_status frg_inspect_geometry(const frg_params *params, const frg_mesh *mesh, 
 frg_status frg_destroy(frg_solver *s) {
   if (!s) return FRG_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  adj_free(s);
   drop_graphs(s);
   double *dp[] = {s->U, s->U0, s->Acc, s->divF[0], s->divF[1], s->divF[2], s->divF[3], s->divF[4], s->detJd,
                   s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
@@ -1210,3 +1216,303 @@ frg_status unfused_update(frg_solver *s) {
   return FRG_OK;
 }
 }  // namespace
+
+// ===================================================================== adjoint
+// Discrete adjoint of frg_update (no counterpart in the reference): a forward
+// run that keeps a checkpoint of U every k steps, then a reverse sweep that,
+// per segment, recomputes the k steps from its checkpoint keeping every RK
+// stage state, and reverses them stage by stage with the adjoint kernels.
+
+struct AdjState {
+  AdjSet ks;
+  double *seed[2] = {nullptr, nullptr};  // stage seeds dJ/d(divF), ping-pong
+  double *lam[2] = {nullptr, nullptr};   // adjoint of a step's final / initial state
+  double *trY = nullptr, *fnbar = nullptr, *ybar = nullptr, *grad = nullptr, *part = nullptr;
+  double *thetaBar = nullptr;
+  double *ckpt = nullptr;    // (nCkpt + 1) states: U at steps 0, k, 2k, ... and U_N last
+  double *stages = nullptr;  // k * nRK stage states of one segment
+  int ckptCap = 0, k = 0, nSteps = 0, stagesCap = 0;  // capacities in states / steps
+  bool gradValid = false;
+};
+
+void adj_free(frg_solver *s) {
+  AdjState *a = s->adj;
+  if (!a) return;
+  double *p[] = {a->seed[0], a->seed[1], a->lam[0], a->lam[1], a->trY, a->fnbar, a->ybar, a->grad, a->part,
+                 a->thetaBar, a->ckpt, a->stages};
+  for (double *q : p) if (q) cudaFree(q);
+  delete a;
+  s->adj = nullptr;
+}
+
+namespace {
+
+// Seed of the last RK stage from the adjoint of a step's final state:
+// gbar = -b_last * dt / detJ * lam.
+__global__ void fr_adj_seed_kernel(const double *lam, const double *detJ, double *seed, double coef, int NV, int NS,
+                                   int nE, int L) {
+  const long n = (long)NV * NS * L;
+  for (long it = blockIdx.x * (long)blockDim.x + threadIdx.x; it < n; it += (long)gridDim.x * blockDim.x) {
+    const int e = (int)(it % L), s = (int)((it / L) % NS);
+    seed[it] = e < nE ? coef * lam[it] / detJ[(size_t)s * L + e] : 0.0;
+  }
+}
+
+bool g_adj_tables[2] = {false, false};
+
+frg_status adj_init(frg_solver *s) {
+  if (s->adj) return FRG_OK;
+  const frg_params &p = s->p;
+  if (p.precision != FRG_FP64) return fail(FRG_ERR_ARG, "adjoint: FP64 precision only");
+  if (p.viscous) return fail(FRG_ERR_ARG, "adjoint: viscous flux not supported");
+  if (!g_adj_tables[p.nDims - 2]) {
+    cudaError_t e = p.nDims == 2 ? upload_tables_adj_2d() : upload_tables_adj_3d();
+    if (e != cudaSuccess) return fail(FRG_ERR_CUDA, "adjoint tables: %s", cudaGetErrorString(e));
+    g_adj_tables[p.nDims - 2] = true;
+  }
+  std::unique_ptr<AdjState> a(new AdjState);
+  KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType, 0};
+  std::string err;
+  const bool ok = p.nDims == 2 ? select_adj_2d(key, a->ks, err) : select_adj_3d(key, a->ks, err);
+  if (!ok) return fail(FRG_ERR_ARG, "%s", err.c_str());
+  const size_t nSE = (size_t)s->nV * s->nS * s->L, nFE = (size_t)s->nV * s->nF * s->L;
+  const size_t nPart = std::max(a->ks.entropyBlocks, (s->nE + 127) / 128);
+  frg_status st;
+  if ((st = dalloc(&a->seed[0], nSE)) || (st = dalloc(&a->seed[1], nSE)) || (st = dalloc(&a->lam[0], nSE)) ||
+      (st = dalloc(&a->lam[1], nSE)) || (st = dalloc(&a->trY, nFE)) || (st = dalloc(&a->fnbar, nFE)) ||
+      (st = dalloc(&a->ybar, nSE)) || (st = dalloc(&a->grad, nSE)) || (st = dalloc(&a->part, nPart)) ||
+      (st = dalloc(&a->thetaBar, 1))) {
+    s->adj = a.release();
+    return st;
+  }
+  s->adj = a.release();
+  return FRG_OK;
+}
+
+AdjArgs adj_args(frg_solver *s, const double *Y, const double *gbar, const double *thetaDir) {
+  AdjArgs a{};
+  a.nE = s->L;
+  a.nEle = s->nE;
+  a.Y = Y;
+  a.gbar = gbar;
+  a.trY = s->adj->trY;
+  a.fnbar = s->adj->fnbar;
+  a.nbr = s->nbr;
+  a.nrm = static_cast<const double *>(s->nrm);
+  a.dA = static_cast<const double *>(s->dAs);
+  a.JG = static_cast<const double *>(s->JG);
+  a.detJ = s->detJd;
+  a.vcjh = s->p.vcjhScheme;
+  a.err = s->err;
+  a.thetaBar = s->adj->thetaBar;
+  for (int i = 0; i < 5; i++) a.thetaDir[i] = thetaDir ? thetaDir[i] : 0.0;
+  a.ph = make_phys(s->p);
+  return a;
+}
+
+frg_status adj_launch(frg_solver *s, const AdjArgs &a) {
+  s->adj->ks.face(a, s->stream);
+  frg_status st = post_launch(s);
+  if (st) return st;
+  s->adj->ks.elem(a, s->stream);
+  return post_launch(s);
+}
+
+// host [spt][ele][field] <-> device [field][spt][ele] state arrays
+frg_status state_to_dev(frg_solver *s, const double *host, double *dev) {
+  frg_status st = ref_scratch(s, 0);
+  if (st) return st;
+  const size_t n = (size_t)s->nV * s->nS * s->nE;
+  CK(cudaMemcpyAsync(s->scratchRef, host, n * 8, cudaMemcpyHostToDevice, s->stream));
+  fr_to_device_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->scratchRef, dev, s->nV, s->nS, s->nE,
+                                                                         s->L);
+  return post_launch(s);
+}
+frg_status state_to_host(frg_solver *s, const double *dev, double *host) {
+  frg_status st = ref_scratch(s, 0);
+  if (st) return st;
+  const size_t n = (size_t)s->nV * s->nS * s->nE;
+  fr_to_ref_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(dev, s->scratchRef, s->nV, s->nS, s->nE, s->L);
+  if ((st = post_launch(s))) return st;
+  CK(cudaMemcpyAsync(host, s->scratchRef, n * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
+// One RK step from Y[0] with the generic stage kernel, keeping every stage
+// state: Y[k] (k = 1..nRK-1) is the state stage k's residual is evaluated at;
+// the step's result goes to Uout.  Same arithmetic as frg_update.
+frg_status step_keep_stages(frg_solver *s, double *const *Y, double *Uout) {
+  s->ks.trace(Y[0], s->tr[0], s->L, s->nE, s->L, s->p.vcjhScheme, s->stream);
+  frg_status st = post_launch(s);
+  if (st) return st;
+  const int nRK = s->nRK;
+  for (int k = 0; k < nRK; k++) {
+    StageArgs a = base_args(s);
+    const bool first = k == 0, last = k == nRK - 1;
+    a.Uin_d = first ? Y[0] : nullptr;
+    a.Uin_s = first ? nullptr : Y[k];
+    a.U0 = Y[0];
+    a.Acc = s->Acc;
+    a.Uout = Uout;
+    a.Wout = last ? nullptr : Y[k + 1];
+    a.trIn = s->tr[k & 1];
+    a.trOut = s->tr[(k + 1) & 1];
+    a.aNext = last ? 0.0 : s->RKa[k + 1];
+    a.bCur = s->RKb[k];
+    a.flags = (last ? SF_LAST : 0) | (first ? SF_FIRST : 0);
+    if ((st = launch_stage_args(s, a))) return st;
+  }
+  s->trValid = false;
+  return FRG_OK;
+}
+
+frg_status adj_check_path(const frg_solver *s) {
+  if (s->p.dtType != 0) return fail(FRG_ERR_ARG, "adjoint: fixed dt (dtType 0) required");
+  if (s->p.timeType == 5) return fail(FRG_ERR_ARG, "adjoint: Jameson-form RK not supported");
+  return FRG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+frg_status frg_objective(frg_solver *s, int kind, double *J, double *grad_host) {
+  if (!s || !J) return fail(FRG_ERR_ARG, "null argument");
+  frg_status st = adj_init(s);
+  if (st) return st;
+  AdjState *a = s->adj;
+  const Phys ph = make_phys(s->p);
+  int nPart = 0;
+  if (kind == FRG_OBJ_ENTROPY) {
+    if (!a->ks.entropy) return fail(FRG_ERR_ARG, "entropy objective needs the Euler equations");
+    a->ks.entropy(s->U, s->detJd, s->wvol, s->nE, s->L, ph, a->grad, a->part, s->stream);
+    nPart = a->ks.entropyBlocks;
+  } else if (kind == FRG_OBJ_WALL_PRESSURE) {
+    if (!a->ks.wallp) return fail(FRG_ERR_ARG, "wall-pressure objective needs the Euler equations");
+    CK(cudaMemsetAsync(a->grad, 0, (size_t)s->nV * s->nS * s->L * 8, s->stream));
+    a->ks.wallp(s->U, s->nbr, s->dAd, s->wsurf, s->p.vcjhScheme, s->nE, s->L, BC_SLIP, ph, a->grad, a->part,
+                s->stream);
+    nPart = (s->nE + 127) / 128;
+  } else {
+    return fail(FRG_ERR_ARG, "unknown objective %d", kind);
+  }
+  if ((st = post_launch(s))) return st;
+  std::vector<double> part(nPart);
+  CK(cudaMemcpyAsync(part.data(), a->part, nPart * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  double t = 0;
+  for (double x : part) t += x;
+  *J = t;
+  a->gradValid = true;
+  if (grad_host) return state_to_host(s, a->grad, grad_host);
+  return FRG_OK;
+}
+
+frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double *thetaDir, double *ubar_host,
+                            double *thetaBar) {
+  if (!s || !gbar_host || !ubar_host) return fail(FRG_ERR_ARG, "null argument");
+  frg_status st = adj_init(s);
+  if (st) return st;
+  AdjState *ad = s->adj;
+  if ((st = state_to_dev(s, gbar_host, ad->seed[0]))) return st;
+  CK(cudaMemsetAsync(ad->thetaBar, 0, 8, s->stream));
+  AdjArgs a = adj_args(s, s->U, ad->seed[0], thetaDir);
+  a.mode = ADJ_PLAIN;
+  a.ybar = ad->ybar;
+  if ((st = adj_launch(s, a))) return st;
+  if (thetaBar) CK(cudaMemcpyAsync(thetaBar, ad->thetaBar, 8, cudaMemcpyDeviceToHost, s->stream));
+  if ((st = state_to_host(s, ad->ybar, ubar_host))) return st;
+  return check_flags(s);
+}
+
+frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery) {
+  if (!s || nsteps < 1 || checkpointEvery < 1) return fail(FRG_ERR_ARG, "bad arguments");
+  frg_status st;
+  if ((st = adj_check_path(s)) || (st = adj_init(s))) return st;
+  AdjState *a = s->adj;
+  const size_t nSE = (size_t)s->nV * s->nS * s->L;
+  const int k = std::min(checkpointEvery, nsteps);
+  const int nCkpt = (nsteps + k - 1) / k;  // checkpoints at 0, k, ..., plus U_N
+  CK(cudaStreamSynchronize(s->stream));
+  if (a->ckpt && a->ckptCap < nCkpt + 1) { cudaFree(a->ckpt); a->ckpt = nullptr; }
+  if (!a->ckpt) {
+    if ((st = dalloc(&a->ckpt, nSE * (nCkpt + 1)))) return st;
+    a->ckptCap = nCkpt + 1;
+  }
+  if (a->stages && a->stagesCap < k) { cudaFree(a->stages); a->stages = nullptr; }
+  if (!a->stages) {
+    if ((st = dalloc(&a->stages, nSE * (size_t)k * s->nRK))) return st;
+    a->stagesCap = k;
+  }
+  a->k = k;
+  a->nSteps = nsteps;
+  for (int n = 0; n < nsteps; n++) {
+    if (n % k == 0)
+      CK(cudaMemcpyAsync(a->ckpt + nSE * (n / k), s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+    if ((st = frg_update(s, 1))) return st;
+  }
+  CK(cudaMemcpyAsync(a->ckpt + nSE * nCkpt, s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
+frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const double *thetaDir, double *lam0_host,
+                                double *thetaBar) {
+  if (!s) return fail(FRG_ERR_ARG, "null handle");
+  AdjState *ad = s->adj;
+  if (!ad || ad->nSteps < 1) return fail(FRG_ERR_ARG, "adjoint: no recorded forward run (frg_adjoint_forward)");
+  frg_status st;
+  const size_t nSE = (size_t)s->nV * s->nS * s->L;
+  const int nRK = s->nRK, k = ad->k, N = ad->nSteps, nCkpt = (N + k - 1) / k;
+  if (lamN_host) {
+    if ((st = state_to_dev(s, lamN_host, ad->lam[0]))) return st;
+  } else {
+    if (!ad->gradValid) return fail(FRG_ERR_ARG, "adjoint: no seed and no objective gradient");
+    CK(cudaMemcpyAsync(ad->lam[0], ad->grad, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  CK(cudaMemsetAsync(ad->thetaBar, 0, 8, s->stream));
+  const double dt = s->p.dt;  // fixed dt (dtType 0)
+  const int nb = (int)std::min<size_t>((nSE + 255) / 256, 148 * 8);
+  fr_adj_seed_kernel<<<nb, 256, 0, s->stream>>>(ad->lam[0], s->detJd, ad->seed[0], -s->RKb[nRK - 1] * dt, s->nV,
+                                                 s->nS, s->nE, s->L);
+  if ((st = post_launch(s))) return st;
+  int cl = 0, cs = 0;  // current lam / seed buffers
+  std::vector<double *> Y(nRK);
+  for (int c = nCkpt - 1; c >= 0; c--) {
+    const int n0 = c * k, m = std::min(k, N - n0);
+    // recompute the segment, keeping every stage state
+    double *seg = ad->stages;
+    CK(cudaMemcpyAsync(seg, ad->ckpt + nSE * c, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+    for (int j = 0; j < m; j++) {
+      for (int q = 0; q < nRK; q++) Y[q] = seg + nSE * ((size_t)j * nRK + q);
+      double *next = j + 1 < m ? seg + nSE * ((size_t)(j + 1) * nRK) : s->U;
+      if ((st = step_keep_stages(s, Y.data(), next))) return st;
+    }
+    // reverse the segment
+    for (int j = m - 1; j >= 0; j--) {
+      for (int q = nRK - 1; q >= 0; q--) {
+        AdjArgs a = adj_args(s, seg + nSE * ((size_t)j * nRK + q), ad->seed[cs], thetaDir);
+        a.mode = ADJ_RK | (q == nRK - 1 ? ADJ_RK_FIRST : 0) | (q == 0 ? ADJ_RK_LAST : 0);
+        a.lam = ad->lam[cl];
+        a.lamNew = ad->lam[cl ^ 1];
+        a.seedOut = ad->seed[cs ^ 1];
+        a.cLam = q == 0 ? s->RKb[nRK - 1] : s->RKb[q - 1];
+        a.cY = q == 0 ? 0.0 : s->RKa[q];
+        a.dt = dt;
+        if ((st = adj_launch(s, a))) return st;
+        cs ^= 1;
+      }
+      cl ^= 1;
+    }
+  }
+  // the solution is the forward run's final state again
+  CK(cudaMemcpyAsync(s->U, ad->ckpt + nSE * nCkpt, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  s->trValid = false;
+  if (thetaBar) CK(cudaMemcpyAsync(thetaBar, ad->thetaBar, 8, cudaMemcpyDeviceToHost, s->stream));
+  if (lam0_host && (st = state_to_host(s, ad->lam[cl], lam0_host))) return st;
+  CK(cudaStreamSynchronize(s->stream));
+  return check_flags(s);
+}
+
+}  // extern "C"

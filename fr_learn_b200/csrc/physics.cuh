@@ -260,22 +260,25 @@ __device__ __forceinline__ void adiabatic_gradient(const R *UL, const R *UR, con
   }
 }
 
-// boundFace::applyBCs for Euler/Navier-Stokes (src/boundFace.cpp:33-277),
-// computed in double.  Returns false for an unknown BC.
-template <int DIM>
-__device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, const Phys &ph) {
-  double rhoR = 0, pR = 0, ER = 0;
-  double vL[3] = {0, 0, 0}, vR[3] = {0, 0, 0};
+// boundFace::applyBCs for Euler/Navier-Stokes (src/boundFace.cpp:33-277).
+// T is double in the solver, a dual number in the adjoint (which also carries
+// the derivative of the boundary state rhoB / vB / pB with respect to a
+// freestream parameter).  Returns false for an unknown BC.
+template <int DIM, typename T>
+__device__ __forceinline__ bool bc_ghost_t(int bc, const T *UL, const double *n, T *UR, const Phys &ph,
+                                           const T &rhoB, const T *vB, const T &pB) {
+  T rhoR = 0, pR = 0, ER = 0;
+  T vL[3] = {0, 0, 0}, vR[3] = {0, 0, 0};
   const double gamma = ph.gamma, gmo = gamma - 1.;
-  double rhoL = UL[0], eL = UL[DIM + 1];
+  T rhoL = UL[0], eL = UL[DIM + 1];
   for (int i = 0; i < DIM; i++) vL[i] = UL[i + 1] / UL[0];
-  double vSq = 0;
+  T vSq = 0;
   for (int i = 0; i < DIM; i++) vSq += (vL[i] * vL[i]);
-  double pL = (gamma - 1.0) * (eL - 0.5 * rhoL * vSq);
+  T pL = (gamma - 1.0) * (eL - 0.5 * rhoL * vSq);
   switch (bc) {
     case BC_SUB_IN:
-      rhoR = ph.rhoB;
-      for (int i = 0; i < DIM; i++) vR[i] = ph.vB[i];
+      rhoR = rhoB;
+      for (int i = 0; i < DIM; i++) vR[i] = vB[i];
       pR = pL;
       vSq = 0;
       for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
@@ -284,15 +287,15 @@ __device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, 
     case BC_SUB_OUT:
       rhoR = rhoL;
       for (int i = 0; i < DIM; i++) vR[i] = vL[i];
-      pR = ph.pB;
+      pR = pB;
       vSq = 0.;
       for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
       ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
       break;
     case BC_SUP_IN:
-      rhoR = ph.rhoB;
-      vR[0] = ph.vB[0]; vR[1] = ph.vB[1]; vR[2] = ph.vB[2];
-      pR = ph.pB;
+      rhoR = rhoB;
+      vR[0] = vB[0]; vR[1] = vB[1]; vR[2] = vB[2];
+      pR = pB;
       vSq = 0.;
       for (int i = 0; i < DIM; i++) vSq += (vR[i] * vR[i]);
       ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
@@ -305,7 +308,7 @@ __device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, 
     case BC_SLIP:
     case BC_SYMMETRY: {
       rhoR = rhoL;
-      double vnL = 0.;
+      T vnL = 0.;
       for (int i = 0; i < DIM; i++) vnL += (vL[i] - 0.0) * n[i];
       for (int i = 0; i < DIM; i++) vR[i] = vL[i] - (2.0) * vnL * n[i];
       ER = eL;
@@ -330,28 +333,28 @@ __device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, 
       ER = (pR / (gamma - 1.0)) + 0.5 * rhoR * vSq;
       break;
     case BC_CHAR: {
-      double vnL = 0., vnB = 0.;
+      T vnL = 0., vnB = 0.;
       for (int i = 0; i < DIM; i++) vnL += vL[i] * n[i];
-      for (int i = 0; i < DIM; i++) vnB += ph.vB[i] * n[i];
-      double cL = sqrt(gamma * pL / rhoL);
-      double cB = sqrt(gamma * ph.pB / ph.rhoB);
-      double R_L, R_B;
+      for (int i = 0; i < DIM; i++) vnB += vB[i] * n[i];
+      T cL = sqrt(gamma * pL / rhoL);
+      T cB = sqrt(gamma * pB / rhoB);
+      T R_L, R_B;
       if (fabs(vnB) >= cB && vnL >= 0) R_L = vnB + 2. / gmo * cB;
       else R_L = vnL + 2. / gmo * cL;
       if (fabs(vnB) >= cB && vnL < 0) R_B = vnL - 2. / gmo * cL;
       else R_B = vnB - 2. / gmo * cB;
-      double rhoFac = .25 * (gamma - 1.) * (R_L - R_B);
-      double rhoBG = rhoFac * rhoFac / gamma;
-      if (vnL < 0) rhoBG *= pow(ph.rhoB, gamma) / ph.pB;
+      T rhoFac = .25 * (gamma - 1.) * (R_L - R_B);
+      T rhoBG = rhoFac * rhoFac / gamma;
+      if (vnL < 0) rhoBG *= pow(rhoB, gamma) / pB;
       else rhoBG *= pow(rhoL, gamma) / pL;
       rhoR = pow(rhoBG, 1. / gmo);
       pR = rhoFac * rhoFac * rhoR / gamma;
-      double VB = 0.5 * (R_L + R_B);
+      T VB = 0.5 * (R_L + R_B);
       for (int i = 0; i < DIM; i++) {
-        if (vnL < 0) vR[i] = ph.vB[i] + (VB - vnB) * n[i];
+        if (vnL < 0) vR[i] = vB[i] + (VB - vnB) * n[i];
         else vR[i] = vL[i] + (VB - vnL) * n[i];
       }
-      double vMag2 = 0;
+      T vMag2 = 0;
       for (int i = 0; i < DIM; i++) vMag2 += vR[i] * vR[i];
       ER = pR / gmo + .5 * rhoR * vMag2;
       break;
@@ -363,6 +366,12 @@ __device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, 
   for (int i = 0; i < DIM; i++) UR[i + 1] = rhoR * vR[i];
   UR[DIM + 1] = ER;
   return true;
+}
+
+template <int DIM>
+__device__ bool bc_ghost(int bc, const double *UL, const double *n, double *UR, const Phys &ph) {
+  const double vB[3] = {ph.vB[0], ph.vB[1], ph.vB[2]};
+  return bc_ghost_t<DIM, double>(bc, UL, n, UR, ph, ph.rhoB, vB, ph.pB);
 }
 
 }  // namespace frg

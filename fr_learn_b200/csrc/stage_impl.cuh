@@ -6,6 +6,7 @@
 #include "dispatch.h"
 #include "kernels.cuh"
 #include "kernels_tma.cuh"
+#include "optab_upload.cuh"
 
 namespace frg {
 namespace {
@@ -133,29 +134,6 @@ bool select_order(const KernelKey &key, KernelSet &k, std::string &err) {
   return false;
 }
 
-template <typename R, typename S>
-cudaError_t upload_tables_impl() {
-  static OpTab<double> hd[4][KMAXP + 1];
-  static OpTab<float> hf[4][KMAXP + 1];
-  for (int sch = 0; sch < 4; sch++)
-    for (int P = 0; P <= KMAXP; P++) {
-      if ((sch == 3 && P < 2) || (sch == 2 && P == 0)) continue;  // eta undefined there
-      Ops1D o = build_ops1d(P, sch);
-      OpTab<double> &d = hd[sch][P];
-      OpTab<float> &f = hf[sch][P];
-      for (int i = 0; i <= KMAXP; i++) {
-        d.lag[0][i] = o.lag[0][i]; d.lag[1][i] = o.lag[1][i];
-        d.gL[i] = o.gL[i]; d.gR[i] = o.gR[i]; d.w[i] = o.w[i];
-        f.lag[0][i] = (float)o.lag[0][i]; f.lag[1][i] = (float)o.lag[1][i];
-        f.gL[i] = (float)o.gL[i]; f.gR[i] = (float)o.gR[i]; f.w[i] = (float)o.w[i];
-        for (int j = 0; j <= KMAXP; j++) { d.dlag[i][j] = o.dlag[i][j]; f.dlag[i][j] = (float)o.dlag[i][j]; }
-      }
-    }
-  cudaError_t e = cudaMemcpyToSymbol(c_opd, hd, sizeof hd);
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_opf, hf, sizeof hf);
-  return e;
-}
-
 }  // namespace
 }  // namespace frg
 
@@ -171,5 +149,5 @@ bool FRG_CAT(select_, FRG_UNIT_NAME)(const KernelKey &key, KernelSet &k, std::st
   err = "unsupported field count";
   return false;
 }
-cudaError_t FRG_CAT(upload_tables_, FRG_UNIT_NAME)() { return upload_tables_impl<FRG_UNIT_R, FRG_UNIT_S>(); }
+cudaError_t FRG_CAT(upload_tables_, FRG_UNIT_NAME)() { return upload_tables_impl(); }
 }  // namespace frg

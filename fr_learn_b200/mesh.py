@@ -204,15 +204,17 @@ def box3d(nx, ny, nz, lo=(-1.0, -1.0, -1.0), hi=(1.0, 1.0, 1.0), bcs=None, pertu
 
 
 def bump2d(nx=96, ny=32, x0=-1.5, x1=1.5, height=0.8, amp=0.0625, width=25.0, cluster=1.5,
-           bc_in="char", bc_out="char", bc_wall="slip_wall"):
+           bc_in="char", bc_out="char", bc_wall="slip_wall", bc_top=None):
     """Channel over a Gaussian bump with 9-node (quadratic) quads.
 
     Lower wall y_w(x) = amp*exp(-width*x^2), upper wall y = height.  Points are
     mapped algebraically, y = y_w(x) + (height - y_w(x)) * s(eta), with the
     wall-clustering stretch s(eta) = 1 + tanh(c(eta-1))/tanh(c), eta in [0,1].
-    Inlet (xmin) / outlet (xmax) take ``bc_in`` / ``bc_out``; both walls
-    ``bc_wall``.
+    Inlet (xmin) / outlet (xmax) take ``bc_in`` / ``bc_out``; the lower wall
+    ``bc_wall``, the upper one ``bc_top`` (default: ``bc_wall``; "symmetry"
+    gives the same ghost state but keeps it out of wall integrals).
     """
+    bc_top = bc_wall if bc_top is None else bc_top
     X = np.linspace(x0, x1, 2 * nx + 1)
     eta = np.linspace(0.0, 1.0, 2 * ny + 1)
     s = 1.0 + np.tanh(cluster * (eta - 1.0)) / np.tanh(cluster)
@@ -238,7 +240,7 @@ def bump2d(nx=96, ny=32, x0=-1.5, x1=1.5, height=0.8, amp=0.0625, width=25.0, cl
             if i == nx - 1:
                 bc[e, 1] = BC[bc_out]
             if j == ny - 1:
-                bc[e, 2] = BC[bc_wall]
+                bc[e, 2] = BC[bc_top]
             if i == 0:
                 bc[e, 3] = BC[bc_in]
             e += 1

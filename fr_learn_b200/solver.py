@@ -101,6 +101,10 @@ def lib():
         "frg_time_stages": ([vp, i, vp, C.c_ulonglong, vp], i),
         "frg_autotune": ([vp, i, C.POINTER(C.c_int), vp], i),
         "frg_set_tile_variant": ([vp, i], i),
+        "frg_objective": ([vp, i, C.POINTER(d), vp], i),
+        "frg_residual_vjp": ([vp, vp, vp, vp, C.POINTER(d)], i),
+        "frg_adjoint_forward": ([vp, i, i], i),
+        "frg_adjoint_backward": ([vp, vp, vp, vp, C.POINTER(d)], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -264,6 +268,53 @@ class Solver:
         out = np.zeros(4)
         _check(lib().frg_autotune(self.h, nsteps, C.byref(v), out.ctypes.data))
         return v.value, out
+
+    # -- discrete adjoint (FP64, inviscid, fixed dt)
+    OBJECTIVES = {"entropy": 1, "wall_pressure": 2}
+
+    def objective(self, kind):
+        """(J, dJ/dU_spts) of the current state; kind "entropy" or "wall_pressure"."""
+        J = C.c_double()
+        g = np.empty(self._shape("U_spts"), np.float64)
+        _check(lib().frg_objective(self.h, self.OBJECTIVES[kind], C.byref(J), g.ctypes.data))
+        return J.value, g
+
+    @staticmethod
+    def _theta(theta_dir):
+        if theta_dir is None:
+            return None, None
+        t = np.ascontiguousarray(theta_dir, np.float64)
+        assert t.shape == (5,)
+        return t, t.ctypes.data
+
+    def residual_vjp(self, gbar, theta_dir=None):
+        """(d divF/dU)^T gbar at the current state, and gbar . d divF/dtheta
+        for the boundary-state direction theta_dir = d(rho, u, v, w, p)_B/dtheta."""
+        g = np.ascontiguousarray(gbar, np.float64)
+        assert g.shape == self._shape("U_spts")
+        out = np.empty_like(g)
+        tb = C.c_double()
+        t, tp = self._theta(theta_dir)
+        _check(lib().frg_residual_vjp(self.h, g.ctypes.data, tp, out.ctypes.data, C.byref(tb)))
+        return out, tb.value
+
+    def adjoint_forward(self, nsteps, checkpoint_every=25):
+        """nsteps of update() keeping checkpoints for adjoint_backward()."""
+        _check(lib().frg_adjoint_forward(self.h, nsteps, checkpoint_every))
+
+    def adjoint_backward(self, lamN=None, theta_dir=None):
+        """(dJ/dU_0, dJ/dtheta through the boundary state) for the last
+        adjoint_forward run; lamN = dJ/dU_N, or None for the last objective()."""
+        lam0 = np.empty(self._shape("U_spts"), np.float64)
+        ptr = None
+        if lamN is not None:
+            lamN = np.ascontiguousarray(lamN, np.float64)
+            assert lamN.shape == lam0.shape
+            ptr = lamN.ctypes.data
+        tb = C.c_double()
+        t, tp = self._theta(theta_dir)
+        _check(lib().frg_adjoint_backward(self.h, ptr, tp, lam0.ctypes.data, C.byref(tb)))
+        return lam0, tb.value
 
     def set_tile_variant(self, v):
         """Select a tile shape of the fused stage kernel by index."""

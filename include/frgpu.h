@@ -207,6 +207,44 @@ frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long
 frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out);
 /* Selects a tile shape of the TMA stage kernel by index (0 = default). */
 frg_status frg_set_tile_variant(frg_solver *s, int variant);
+/* ---- Discrete adjoint (no counterpart in the reference) ----------------
+ * FP64, inviscid (Euler or advection), fixed dt (dtType 0), RK tables of
+ * timeType 0/2/4.  The adjoint kernels transpose the residual operation by
+ * operation (operators, flux Jacobians, Rusanov / Roe / Lax-Friedrichs and
+ * the boundary ghost states through dual numbers). */
+
+/* Objectives of the current state.  FRG_OBJ_ENTROPY: sum over solution
+ * points of w detJ (p rhoBound^gamma / (rho^gamma pBound) - 1)
+ * (integrateError's entropy error, src/solver.cpp:1507-1531).
+ * FRG_OBJ_WALL_PRESSURE: pressure integrated over the slip-wall faces with
+ * computeWallForce's face quadrature (src/boundFace.cpp:330-378), from the
+ * elements' traces.  J receives the value; grad_host (may be NULL) dJ/dU at
+ * the solution points, [spt][ele][field].  The gradient is kept as the
+ * default seed of frg_adjoint_backward. */
+enum { FRG_OBJ_ENTROPY = 1, FRG_OBJ_WALL_PRESSURE = 2 };
+frg_status frg_objective(frg_solver *s, int kind, double *J, double *grad_host);
+
+/* Vector-Jacobian product of calcResidual at the current state: given
+ * gbar = dJ/d(divF) ([spt][ele][field]), ubar = (d divF / dU)^T gbar.
+ * thetaDir (5 doubles, may be NULL) is the derivative of the boundary state
+ * (rhoBound, uBound, vBound, wBound, pBound) with respect to a scalar
+ * parameter theta; thetaBar receives gbar . d(divF)/d(theta). */
+frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double *thetaDir, double *ubar_host,
+                            double *thetaBar);
+
+/* Forward run of nsteps frg_update steps keeping a checkpoint of U every
+ * checkpointEvery steps (device memory: nsteps/checkpointEvery + 2 states,
+ * plus checkpointEvery x nRK stage states for the reverse sweep). */
+frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery);
+/* Reverse sweep of the last frg_adjoint_forward run: from lamN = dJ/dU_N
+ * ([spt][ele][field]; NULL = the gradient of the last frg_objective call)
+ * to lam0 = dJ/dU_0 and thetaBar = dJ/dtheta through the boundary state
+ * (the initial state's own dependence on theta is lam0 . dU_0/dtheta).
+ * Each segment between checkpoints is recomputed with its RK stage states,
+ * then reversed stage by stage.  The solution is left at U_N. */
+frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const double *thetaDir, double *lam0_host,
+                                double *thetaBar);
+
 /* Device-side launch counter: kernels launched by this handle so far. */
 frg_status frg_launch_count(const frg_solver *s, long long *count);
 
