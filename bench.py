@@ -236,7 +236,88 @@ def run_gpu(args, rank, world, local_rank):
     state_bytes = s.nSpts * s.nEles * s.nFields * 8
     for sv in solvers.values():
         sv.set_stream(None)
+    res["adjoint"] = run_adjoint_bump(stream)
     return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
+
+
+def run_adjoint_bump(stream, nsteps=500, every=25):
+    """Adjoint workload: 2D Euler channel over a Gaussian bump (96x32
+    quadratic quads clustered to the wall, P=3, Roe, char inlet/outlet at
+    Mach 0.5, slip lower wall, symmetry top), freestream initial state, RK4
+    with the CFL-0.5 dt of the first step held fixed, 500 steps; J = pressure
+    integral over the lower wall at the final time; gradients dJ/dU_0 and
+    dJ/dMach by the reverse RK sweep with checkpoints every 25 steps.
+    Returns forward and adjoint times per step (CUDA events)."""
+    import torch
+
+    from fr_learn_b200 import Solver, bump2d
+
+    g = 1.4
+    c = np.sqrt(g)
+    M = 0.5
+    mesh = bump2d(96, 32, bc_top="symmetry")
+    kw = dict(order=3, riemannType=1, timeType=4, uBound=M * c, pBound=1.0, rhoBound=1.0)
+    s0 = Solver(mesh, dtType=1, CFL=0.5, **kw)
+    s0.setInitialCondition(0)
+    s0.update(1)
+    dt = s0.dt
+
+    def make(Mach):
+        s = Solver(mesh, dtType=0, dt=dt, **dict(kw, uBound=Mach * c))
+        s.set_stream(stream.cuda_stream)
+        s.setInitialCondition(0)
+        return s
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            r = fn()
+            b.record(stream)
+            b.synchronize()
+        return a.elapsed_time(b), r
+
+    s = make(M)
+    s.update(3)  # warm-up (graphs, kernels)
+    s.setInitialCondition(0)
+    fwd_ms, _ = timed(lambda: s.update(nsteps))
+    s.setInitialCondition(0)
+    U0 = s.get("U_spts")
+    rec_ms, _ = timed(lambda: s.adjoint_forward(nsteps, every))
+    J, _ = s.objective("wall_pressure")
+    theta = np.array([0.0, c, 0.0, 0.0, 0.0])
+    adj_ms, (lam0, tbar) = timed(lambda: s.adjoint_backward(None, theta))
+    # the same gradient with every stage state kept by the forward run
+    # (nsteps x 4 states in HBM; the reverse sweep recomputes nothing)
+    s.setInitialCondition(0)
+    keep_fwd_ms, _ = timed(lambda: s.adjoint_forward(nsteps, 0))
+    s.objective("wall_pressure")
+    keep_ms, (lam0k, tbark) = timed(lambda: s.adjoint_backward(None, theta))
+    rho = U0[..., 0]
+    dU = np.zeros_like(U0)
+    dU[..., 1] = rho * c
+    dU[..., 3] = U0[..., 1] * c
+    dJdM = float(np.sum(lam0 * dU)) + tbar
+    # central difference of the forward solver over the Mach number
+    eps = 1e-6
+    Jpm = []
+    for sg in (1, -1):
+        s2 = make(M + sg * eps)
+        s2.update(nsteps)
+        Jpm.append(s2.objective("wall_pressure")[0])
+        s2.set_stream(None)
+    s.set_stream(None)
+    fd = (Jpm[0] - Jpm[1]) / (2 * eps)
+    return {"workload": "euler2d_bump_channel_96x32_q9_P3_roe_char_slip_M0.5_rk44_500steps",
+            "steps": nsteps, "checkpoint_every": every, "dt": dt, "dof": s.nEles * s.nSpts * s.nFields,
+            "forward_ms_per_step": fwd_ms / nsteps, "forward_with_checkpoints_ms_per_step": rec_ms / nsteps,
+            "adjoint_ms_per_step": adj_ms / nsteps, "adjoint_over_forward": adj_ms / fwd_ms,
+            "keep_all_stages": {"forward_ms_per_step": keep_fwd_ms / nsteps,
+                                "adjoint_ms_per_step": keep_ms / nsteps, "adjoint_over_forward": keep_ms / fwd_ms,
+                                "max_rel_diff_vs_checkpointed": float(np.abs(lam0k - lam0).max()
+                                                                      / np.abs(lam0).max())},
+            "J_wall_pressure": J, "dJ_dMach": dJdM, "dJ_dMach_central_difference": fd,
+            "dJ_dMach_rel_diff": abs(dJdM - fd) / abs(fd)}
 
 
 def cpu_baseline(steps=2, threads=1):
@@ -366,6 +447,7 @@ def main():
                 "d2h_bytes_per_step": state_bytes,
                 "how": "frg_update_host per step: pinned host state [spt][ele][field] -> device, one RK4 step, "
                        "state -> host"},
+        "adjoint": res["adjoint"],
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }

@@ -52,7 +52,7 @@ struct AdjArgs {
   double cLam, cY;        // seedOut = -(cLam * base + cY * ybar) * dt / detJ
   double dt;
   int mode;               // ADJ_* flags
-  double thetaDir[5];     // d(rhoB, vB[0..2], pB) / d(theta) of the boundary state
+  const double *thetaDir; // d(rhoB, vB[0..2], pB) / d(theta) of the boundary state (device, 5)
   double *thetaBar;       // += fbar . dFn/dtheta over boundary flux points
   Phys ph;
 };
@@ -111,8 +111,11 @@ __global__ void __launch_bounds__(256) fr_adj_face_kernel(const AdjArgs a) {
 template <class C>
 struct AdjTile {
   static constexpr int PER_ELE = (2 * C::NV * C::NS + 2 * C::NV * C::NF) * 8;
-  static constexpr int TE = (16 * PER_ELE <= 64 * 1024) ? 16 : (8 * PER_ELE <= 64 * 1024) ? 8
-                            : (4 * PER_ELE <= 64 * 1024) ? 4 : (2 * PER_ELE <= 64 * 1024) ? 2 : 1;
+  // at most 8 elements per block: the dual-number Jacobians hold ~255
+  // registers per thread (two blocks per SM), so small tiles keep every SM
+  // busy on meshes of a few thousand elements
+  static constexpr int TE = (8 * PER_ELE <= 64 * 1024) ? 8 : (4 * PER_ELE <= 64 * 1024) ? 4
+                            : (2 * PER_ELE <= 64 * 1024) ? 2 : 1;
   static constexpr int NT = 128;
   static constexpr int SMEM = TE * PER_ELE;
 };

@@ -8,7 +8,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <array>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -179,6 +181,7 @@ using namespace frg;
 
 struct AdjState;  // discrete-adjoint buffers (end of this file)
 void adj_free(frg_solver *s);
+void adj_forget_graphs(frg_solver *s);
 
 // -------------------------------------------------------------- the handle
 struct frg_solver {
@@ -439,6 +442,7 @@ frg_status launch_wavesp(frg_solver *s) {
 }
 
 void drop_graphs(frg_solver *s) {
+  adj_forget_graphs(s);
   for (auto &r : s->graph)
     for (auto &q : r)
       for (auto &g : q)
@@ -1229,17 +1233,33 @@ struct AdjState {
   double *lam[2] = {nullptr, nullptr};   // adjoint of a step's final / initial state
   double *trY = nullptr, *fnbar = nullptr, *ybar = nullptr, *grad = nullptr, *part = nullptr;
   double *thetaBar = nullptr;
+  double *thetaDir = nullptr;  // 5 doubles, device
   double *ckpt = nullptr;    // (nCkpt + 1) states: U at steps 0, k, 2k, ... and U_N last
   double *stages = nullptr;  // k * nRK stage states of one segment
   int ckptCap = 0, k = 0, nSteps = 0, stagesCap = 0;  // capacities in states / steps
+  bool keepAll = false;  // the forward run kept every stage state
+  // captured per-segment work of the reverse sweep, keyed by (kind, segment
+  // length, buffer parities); valid while the buffers they name stay
+  struct Captured {
+    cudaGraphExec_t exec;
+    int launches;
+  };
+  std::map<std::array<int, 4>, Captured> graphs;
   bool gradValid = false;
 };
+
+void adj_forget_graphs(frg_solver *s) {
+  if (!s->adj) return;
+  for (auto &g : s->adj->graphs) cudaGraphExecDestroy(g.second.exec);
+  s->adj->graphs.clear();
+}
 
 void adj_free(frg_solver *s) {
   AdjState *a = s->adj;
   if (!a) return;
+  for (auto &g : a->graphs) cudaGraphExecDestroy(g.second.exec);
   double *p[] = {a->seed[0], a->seed[1], a->lam[0], a->lam[1], a->trY, a->fnbar, a->ybar, a->grad, a->part,
-                 a->thetaBar, a->ckpt, a->stages};
+                 a->thetaBar, a->thetaDir, a->ckpt, a->stages};
   for (double *q : p) if (q) cudaFree(q);
   delete a;
   s->adj = nullptr;
@@ -1281,7 +1301,7 @@ frg_status adj_init(frg_solver *s) {
   if ((st = dalloc(&a->seed[0], nSE)) || (st = dalloc(&a->seed[1], nSE)) || (st = dalloc(&a->lam[0], nSE)) ||
       (st = dalloc(&a->lam[1], nSE)) || (st = dalloc(&a->trY, nFE)) || (st = dalloc(&a->fnbar, nFE)) ||
       (st = dalloc(&a->ybar, nSE)) || (st = dalloc(&a->grad, nSE)) || (st = dalloc(&a->part, nPart)) ||
-      (st = dalloc(&a->thetaBar, 1))) {
+      (st = dalloc(&a->thetaBar, 1)) || (st = dalloc(&a->thetaDir, 5))) {
     s->adj = a.release();
     return st;
   }
@@ -1289,7 +1309,7 @@ frg_status adj_init(frg_solver *s) {
   return FRG_OK;
 }
 
-AdjArgs adj_args(frg_solver *s, const double *Y, const double *gbar, const double *thetaDir) {
+AdjArgs adj_args(frg_solver *s, const double *Y, const double *gbar) {
   AdjArgs a{};
   a.nE = s->L;
   a.nEle = s->nE;
@@ -1305,7 +1325,7 @@ AdjArgs adj_args(frg_solver *s, const double *Y, const double *gbar, const doubl
   a.vcjh = s->p.vcjhScheme;
   a.err = s->err;
   a.thetaBar = s->adj->thetaBar;
-  for (int i = 0; i < 5; i++) a.thetaDir[i] = thetaDir ? thetaDir[i] : 0.0;
+  a.thetaDir = s->adj->thetaDir;
   a.ph = make_phys(s->p);
   return a;
 }
@@ -1316,6 +1336,35 @@ frg_status adj_launch(frg_solver *s, const AdjArgs &a) {
   if (st) return st;
   s->adj->ks.elem(a, s->stream);
   return post_launch(s);
+}
+
+void adj_drop_graphs(AdjState *a) {
+  for (auto &g : a->graphs) cudaGraphExecDestroy(g.second.exec);
+  a->graphs.clear();
+}
+
+// Runs `enqueue` through a CUDA graph captured on first use under `key`.
+template <class F>
+frg_status adj_replay(frg_solver *s, const std::array<int, 4> &key, F enqueue) {
+  auto &gs = s->adj->graphs;
+  auto it = gs.find(key);
+  if (it == gs.end()) {
+    const long long before = s->launches;
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    frg_status st = enqueue();
+    cudaError_t ce = cudaStreamEndCapture(s->stream, &gr);
+    if (st) return st;
+    if (ce != cudaSuccess) return fail(FRG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    cudaGraphExec_t ex;
+    CK(cudaGraphInstantiate(&ex, gr, 0));
+    CK(cudaGraphDestroy(gr));
+    it = gs.emplace(key, AdjState::Captured{ex, (int)(s->launches - before)}).first;
+    s->launches = before;
+  }
+  CK(cudaGraphLaunch(it->second.exec, s->stream));
+  s->launches += it->second.launches;
+  return FRG_OK;
 }
 
 // host [spt][ele][field] <-> device [field][spt][ele] state arrays
@@ -1339,31 +1388,60 @@ frg_status state_to_host(frg_solver *s, const double *dev, double *host) {
   return FRG_OK;
 }
 
-// One RK step from Y[0] with the generic stage kernel, keeping every stage
-// state: Y[k] (k = 1..nRK-1) is the state stage k's residual is evaluated at;
-// the step's result goes to Uout.  Same arithmetic as frg_update.
-frg_status step_keep_stages(frg_solver *s, double *const *Y, double *Uout) {
-  s->ks.trace(Y[0], s->tr[0], s->L, s->nE, s->L, s->p.vcjhScheme, s->stream);
-  frg_status st = post_launch(s);
-  if (st) return st;
+// One RK step from U (on entry U_n, on exit U_{n+1}) keeping every stage
+// state: Y[0] receives a copy of U_n and Y[k] (k = 1..nRK-1) the state stage
+// k's residual is evaluated at.  Same kernels and arithmetic as frg_update:
+// the TMA stage kernel where the update uses it (stage states through tensor
+// maps made for the Y slots), else the generic one.  Traces of U must be
+// current on entry (tr[curTr]) and are current on exit.
+frg_status step_keep_stages(frg_solver *s, double *const *Y, bool advanceTime = false) {
+  const size_t nSE = (size_t)s->nV * s->nS * s->L;
+  CK(cudaMemcpyAsync(Y[0], s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+  frg_status st;
   const int nRK = s->nRK;
+  CUtensorMap mY[8];
+  if (s->useTma)
+    for (int k = 1; k < nRK; k++)
+      if ((st = make_map(&mY[k], Y[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, s->nV * s->nS, s->L,
+                         s->ks.tma[s->tmaVar].TE)))
+        return st;
   for (int k = 0; k < nRK; k++) {
     StageArgs a = base_args(s);
     const bool first = k == 0, last = k == nRK - 1;
-    a.Uin_d = first ? Y[0] : nullptr;
-    a.Uin_s = first ? nullptr : Y[k];
-    a.U0 = Y[0];
-    a.Acc = s->Acc;
-    a.Uout = Uout;
-    a.Wout = last ? nullptr : Y[k + 1];
-    a.trIn = s->tr[k & 1];
-    a.trOut = s->tr[(k + 1) & 1];
+    a.trIn = s->tr[s->curTr];
+    a.trOut = s->tr[s->curTr ^ 1];
     a.aNext = last ? 0.0 : s->RKa[k + 1];
     a.bCur = s->RKb[k];
-    a.flags = (last ? SF_LAST : 0) | (first ? SF_FIRST : 0);
-    if ((st = launch_stage_args(s, a))) return st;
+    a.flags = (last ? SF_LAST : 0) | (first ? SF_FIRST : 0) | (last && advanceTime ? SF_TIME : 0);
+    a.Acc = s->Acc;
+    if (s->useTma) {
+      a.Uin_d = first ? s->U : nullptr;
+      a.Uin_s = first ? nullptr : Y[k];
+      TmaMaps mm;
+      mm.U = s->mU;
+      mm.Acc = s->mAcc;
+      mm.Win = first ? s->mW[0] : mY[k];
+      mm.Wout = last ? s->mW[0] : mY[k + 1];
+      mm.trOut = s->mTr[s->curTr ^ 1];
+      mm.JG = s->mJG;
+      mm.det = s->mDet;
+      mm.nrm = s->mNrm;
+      mm.dA = s->mDA;
+      mm.nbr = s->mNbr;
+      const KernelSet::TmaVariant &tv = s->ks.tma[s->tmaVar];
+      tv.launch(&a, &mm, s->nBlkTma, tv.smem, s->stream);
+      st = post_launch(s);
+    } else {
+      a.Uin_d = first ? Y[0] : nullptr;
+      a.Uin_s = first ? nullptr : Y[k];
+      a.U0 = Y[0];
+      a.Uout = s->U;
+      a.Wout = last ? nullptr : Y[k + 1];
+      st = launch_stage_args(s, a);
+    }
+    if (st) return st;
+    s->curTr ^= 1;
   }
-  s->trValid = false;
   return FRG_OK;
 }
 
@@ -1417,7 +1495,9 @@ frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double
   AdjState *ad = s->adj;
   if ((st = state_to_dev(s, gbar_host, ad->seed[0]))) return st;
   CK(cudaMemsetAsync(ad->thetaBar, 0, 8, s->stream));
-  AdjArgs a = adj_args(s, s->U, ad->seed[0], thetaDir);
+  const double zero[5] = {0, 0, 0, 0, 0};
+  CK(cudaMemcpy(ad->thetaDir, thetaDir ? thetaDir : zero, 5 * 8, cudaMemcpyHostToDevice));
+  AdjArgs a = adj_args(s, s->U, ad->seed[0]);
   a.mode = ADJ_PLAIN;
   a.ybar = ad->ybar;
   if ((st = adj_launch(s, a))) return st;
@@ -1427,14 +1507,17 @@ frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double
 }
 
 frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery) {
-  if (!s || nsteps < 1 || checkpointEvery < 1) return fail(FRG_ERR_ARG, "bad arguments");
+  if (!s || nsteps < 1 || checkpointEvery < 0) return fail(FRG_ERR_ARG, "bad arguments");
   frg_status st;
   if ((st = adj_check_path(s)) || (st = adj_init(s))) return st;
   AdjState *a = s->adj;
   const size_t nSE = (size_t)s->nV * s->nS * s->L;
-  const int k = std::min(checkpointEvery, nsteps);
+  // checkpointEvery 0: keep every stage state of the run (no recomputation)
+  const bool keepAll = checkpointEvery == 0;
+  const int k = keepAll ? nsteps : std::min(checkpointEvery, nsteps);
   const int nCkpt = (nsteps + k - 1) / k;  // checkpoints at 0, k, ..., plus U_N
   CK(cudaStreamSynchronize(s->stream));
+  adj_drop_graphs(a);  // they name the stage slots of the last run's layout
   if (a->ckpt && a->ckptCap < nCkpt + 1) { cudaFree(a->ckpt); a->ckpt = nullptr; }
   if (!a->ckpt) {
     if ((st = dalloc(&a->ckpt, nSE * (nCkpt + 1)))) return st;
@@ -1447,14 +1530,27 @@ frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery) {
   }
   a->k = k;
   a->nSteps = nsteps;
-  for (int n = 0; n < nsteps; n++) {
-    if (n % k == 0)
+  a->keepAll = keepAll;
+  if (keepAll) {
+    CK(cudaMemcpyAsync(a->ckpt, s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+    if ((st = ensure_traces(s))) return st;
+    std::vector<double *> Y(s->nRK);
+    for (int n = 0; n < nsteps; n++) {
+      for (int q = 0; q < s->nRK; q++) Y[q] = a->stages + nSE * ((size_t)n * s->nRK + q);
+      if ((st = step_keep_stages(s, Y.data(), true))) return st;
+      s->iter++;
+    }
+    s->trValid = true;
+    s->dtFresh = false;
+  } else {
+    for (int n = 0; n < nsteps; n += k) {
       CK(cudaMemcpyAsync(a->ckpt + nSE * (n / k), s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
-    if ((st = frg_update(s, 1))) return st;
+      if ((st = frg_update(s, std::min(k, nsteps - n)))) return st;
+    }
   }
   CK(cudaMemcpyAsync(a->ckpt + nSE * nCkpt, s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  return FRG_OK;
+  return check_flags(s);
 }
 
 frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const double *thetaDir, double *lam0_host,
@@ -1472,39 +1568,65 @@ frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const do
     CK(cudaMemcpyAsync(ad->lam[0], ad->grad, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
   }
   CK(cudaMemsetAsync(ad->thetaBar, 0, 8, s->stream));
+  const double zero[5] = {0, 0, 0, 0, 0};
+  CK(cudaMemcpy(ad->thetaDir, thetaDir ? thetaDir : zero, 5 * 8, cudaMemcpyHostToDevice));
   const double dt = s->p.dt;  // fixed dt (dtType 0)
   const int nb = (int)std::min<size_t>((nSE + 255) / 256, 148 * 8);
   fr_adj_seed_kernel<<<nb, 256, 0, s->stream>>>(ad->lam[0], s->detJd, ad->seed[0], -s->RKb[nRK - 1] * dt, s->nV,
                                                  s->nS, s->nE, s->L);
   if ((st = post_launch(s))) return st;
   int cl = 0, cs = 0;  // current lam / seed buffers
-  std::vector<double *> Y(nRK);
+  double *seg = ad->stages;
   for (int c = nCkpt - 1; c >= 0; c--) {
     const int n0 = c * k, m = std::min(k, N - n0);
-    // recompute the segment, keeping every stage state
-    double *seg = ad->stages;
-    CK(cudaMemcpyAsync(seg, ad->ckpt + nSE * c, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
-    for (int j = 0; j < m; j++) {
-      for (int q = 0; q < nRK; q++) Y[q] = seg + nSE * ((size_t)j * nRK + q);
-      double *next = j + 1 < m ? seg + nSE * ((size_t)(j + 1) * nRK) : s->U;
-      if ((st = step_keep_stages(s, Y.data(), next))) return st;
+    // recompute the segment from its checkpoint, keeping every stage state
+    // (already kept when the forward run stored them all); one captured
+    // graph per segment length and trace-buffer parity
+    if (!ad->keepAll) {
+      CK(cudaMemcpyAsync(s->U, ad->ckpt + nSE * c, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+      s->trValid = false;
+      if ((st = ensure_traces(s))) return st;
+      const int tr0 = s->curTr;
+      st = adj_replay(s, {0, m, tr0, 0}, [&]() {
+        std::vector<double *> Y(nRK);
+        for (int j = 0; j < m; j++) {
+          for (int q = 0; q < nRK; q++) Y[q] = seg + nSE * ((size_t)j * nRK + q);
+          frg_status e = step_keep_stages(s, Y.data());
+          if (e) return e;
+        }
+        return FRG_OK;
+      });
+      if (st) return st;
+      s->curTr = tr0 ^ ((m * nRK) & 1);
     }
-    // reverse the segment
-    for (int j = m - 1; j >= 0; j--) {
-      for (int q = nRK - 1; q >= 0; q--) {
-        AdjArgs a = adj_args(s, seg + nSE * ((size_t)j * nRK + q), ad->seed[cs], thetaDir);
-        a.mode = ADJ_RK | (q == nRK - 1 ? ADJ_RK_FIRST : 0) | (q == 0 ? ADJ_RK_LAST : 0);
-        a.lam = ad->lam[cl];
-        a.lamNew = ad->lam[cl ^ 1];
-        a.seedOut = ad->seed[cs ^ 1];
-        a.cLam = q == 0 ? s->RKb[nRK - 1] : s->RKb[q - 1];
-        a.cY = q == 0 ? 0.0 : s->RKa[q];
-        a.dt = dt;
-        if ((st = adj_launch(s, a))) return st;
-        cs ^= 1;
+    // reverse the segment, stage by stage (captured when checkpointed: the
+    // same slots serve every segment; a kept-all run is reversed once, launch
+    // by launch)
+    const int cl0 = cl, cs0 = cs;
+    auto reverse = [&]() {
+      int l = cl0, q2 = cs0;
+      for (int j = m - 1; j >= 0; j--) {
+        for (int q = nRK - 1; q >= 0; q--) {
+          AdjArgs a = adj_args(s, seg + nSE * ((size_t)j * nRK + q), ad->seed[q2]);
+          a.mode = ADJ_RK | (q == nRK - 1 ? ADJ_RK_FIRST : 0) | (q == 0 ? ADJ_RK_LAST : 0);
+          a.lam = ad->lam[l];
+          a.lamNew = ad->lam[l ^ 1];
+          a.seedOut = ad->seed[q2 ^ 1];
+          a.cLam = q == 0 ? s->RKb[nRK - 1] : s->RKb[q - 1];
+          a.cY = q == 0 ? 0.0 : s->RKa[q];
+          a.dt = dt;
+          frg_status e = adj_launch(s, a);
+          if (e) return e;
+          q2 ^= 1;
+        }
+        l ^= 1;
       }
-      cl ^= 1;
-    }
+      return FRG_OK;
+    };
+    st = ad->keepAll ? reverse() : adj_replay(s, {1, m, cl0, cs0}, reverse);
+    if (st) return st;
+    cs = cs0 ^ ((m * nRK) & 1);
+    cl = cl0 ^ (m & 1);
   }
   // the solution is the forward run's final state again
   CK(cudaMemcpyAsync(s->U, ad->ckpt + nSE * nCkpt, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));

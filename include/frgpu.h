@@ -234,7 +234,9 @@ frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double
 
 /* Forward run of nsteps frg_update steps keeping a checkpoint of U every
  * checkpointEvery steps (device memory: nsteps/checkpointEvery + 2 states,
- * plus checkpointEvery x nRK stage states for the reverse sweep). */
+ * plus checkpointEvery x nRK stage states for the reverse sweep).
+ * checkpointEvery 0 keeps every RK stage state of the run instead
+ * (nsteps x nRK states), so the reverse sweep recomputes nothing. */
 frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery);
 /* Reverse sweep of the last frg_adjoint_forward run: from lamN = dJ/dU_N
  * ([spt][ele][field]; NULL = the gradient of the last frg_objective call)

@@ -103,11 +103,12 @@ def _freestream_dU_dM(U0, c):
     return d
 
 
-@pytest.mark.parametrize("timeType,nsteps,every", [(4, 7, 3), (2, 5, 5), (0, 4, 2)])
+@pytest.mark.parametrize("timeType,nsteps,every", [(4, 7, 3), (2, 5, 5), (0, 4, 2), (4, 6, 0)])
 def test_adjoint_rk_matches_central_differences(timeType, nsteps, every):
     """Bump channel (P=2, Roe, char inlet/outlet, slip lower wall, symmetry
     top), J = wall pressure integral after nsteps; gradients with respect to
-    the initial state (a random direction) and to the freestream Mach number."""
+    the initial state (a random direction) and to the freestream Mach number.
+    every = 0: the forward run keeps all stage states (no recomputation)."""
     from fr_learn_b200 import bump2d
 
     c = np.sqrt(GAMMA)
@@ -125,6 +126,7 @@ def test_adjoint_rk_matches_central_differences(timeType, nsteps, every):
     s2 = _solver(mesh, 0, **kw)
     s2.update(nsteps)
     assert relerr(s.get("U_spts"), s2.get("U_spts")) < 1e-13
+    assert s.time == pytest.approx(s2.time, rel=1e-14)
 
     rng = np.random.default_rng(11)
     delta = rng.standard_normal(U0.shape) * np.abs(U0).max(axis=(0, 1), keepdims=True)
@@ -223,3 +225,19 @@ def test_autograd_binding_matches_central_differences():
     fd = (Lp[0] - Lp[1]) / (2 * eps)
     adj = float(np.sum(g * delta))
     assert abs(fd - adj) <= 1e-6 * abs(adj), (fd, adj)
+
+
+def test_checkpointed_and_stored_sweeps_agree():
+    """Checkpoint intervals 1, 3 and 'keep everything' give the same dJ/dU_0."""
+    from fr_learn_b200 import bump2d
+
+    c = np.sqrt(GAMMA)
+    mesh = bump2d(6, 3, bc_top="symmetry")
+    kw = dict(order=3, riemannType=1, uBound=0.5 * c, pBound=1.0)
+    out = []
+    for every in (1, 3, 0):
+        s = _solver(mesh, 0, **kw)
+        s.adjoint_forward(8, every)
+        s.objective("wall_pressure")
+        out.append(s.adjoint_backward(None, np.array([0.0, c, 0, 0, 0]))[0])
+    assert relerr(out[1], out[0]) < 1e-12 and relerr(out[2], out[0]) < 1e-12
