@@ -53,6 +53,8 @@ struct AdjArgs {
   double dt;
   int mode;               // ADJ_* flags
   const double *thetaDir; // d(rhoB, vB[0..2], pB) / d(theta) of the boundary state (device, 5)
+  const int *grp;         // ensemble mode: group of each element, else null
+  const double *dtGrp;    // ensemble mode: fixed dt per group (replaces dt)
   double *thetaBar;       // += fbar . dFn/dtheta over boundary flux points
   Phys ph;
 };
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(128) fr_adj_elem_kernel(const AdjArgs a) {
         const double base = (a.mode & ADJ_RK_FIRST) ? a.lam[gi] : a.lamNew[gi];
         const double ln = base + yb;
         a.lamNew[gi] = ln;
-        const double D = a.dt * idet;
+        const double D = (a.grp ? a.dtGrp[a.grp[eg]] : a.dt) * idet;
         if (a.mode & ADJ_RK_LAST) a.seedOut[gi] = -a.cLam * ln * D;
         else a.seedOut[gi] = -(a.cLam * a.lam[gi] + a.cY * yb) * D;
       }

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256) fr_dt_kernel(const double *__restrict__ w
                                                     const double *__restrict__ vol, const double *__restrict__ wsurf,
                                                     int NF, int NFF, int nE, int L, double cflFac, double *eleDt,
                                                     double *blockMin, unsigned *ticket, double *dtOut,
-                                                    unsigned *err) {
+                                                    unsigned *err, const int *grp) {
   __shared__ double part[kDtSlices][32];
   __shared__ double wmin[32];
   __shared__ bool last;
@@ -56,7 +56,13 @@ __global__ void __launch_bounds__(256) fr_dt_kernel(const double *__restrict__ w
       const double dte = cflFac * vol[e] / iw;  // (CFL * limit * 2) * vol / intWave
       eleDt[e] = dte;
       my = dte;
+      if (grp) {  // ensemble mode: the minimum per group (dtOut preset to a huge value)
+        if (!(dte > 1e-13)) atomicOr(err, ERRF_DT);
+        else atomicMin(reinterpret_cast<unsigned long long *>(dtOut + grp[e]),
+                       (unsigned long long)__double_as_longlong(dte));
+      }
     }
+    if (grp) return;
     for (int o = 16; o > 0; o >>= 1) {
       const double t = __shfl_xor_sync(0xffffffffu, my, o);
       my = (isnan(t) || t < my) ? t : my;
@@ -87,6 +93,16 @@ __global__ void __launch_bounds__(256) fr_dt_kernel(const double *__restrict__ w
     if (isnan(r) || r < 1e-13) atomicOr(err, ERRF_DT);
     *ticket = 0;
   }
+}
+
+// Ensemble mode, once per step before the stages: each group's time advances
+// by the dt its elements use this step, and the slot the last stage
+// minimises the next dt into is reset.
+__global__ void fr_group_step_kernel(const double *dtCur, double *dtNext, double *time, int nGrp) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nGrp) return;
+  time[g] += dtCur[g];
+  if (dtNext) dtNext[g] = __longlong_as_double(0x7f7f7f7f7f7f7f7fLL);
 }
 
 __global__ void fr_timestep_kernel(double *U, const double *U0, const double *divF, const double *detJ,
@@ -204,6 +220,11 @@ struct frg_solver {
   double *detJd = nullptr, *nrmOwn = nullptr, *dAd = nullptr, *vol = nullptr, *wsurf = nullptr, *wvol = nullptr;
   int *nbr = nullptr;
   double *waveSp = nullptr, *eleDt = nullptr, *dtDev = nullptr, *timeDev = nullptr, *blockMin = nullptr;
+  // ensemble mode (frg_set_groups): independent cases in one mesh, each
+  // with its own dt (two slots of nGrp) and time
+  int *grp = nullptr;
+  int nGrp = 0;
+  double *grpDt = nullptr, *grpTime = nullptr;
   int dtCur = 0;  // slot of dtDev[2] holding the current step's dt (two slots
                   // when the last stage computes the next step's dt)
   int dtLast = 0;  // slot of the dt the last step used or frg_calc_dt computed
@@ -328,6 +349,11 @@ frg_status ensure_traces(frg_solver *s) {
   return FRG_OK;
 }
 
+// dt slot `slot` (0/1): a scalar, or one value per group in ensemble mode
+double *dt_slot(frg_solver *s, int slot) {
+  return s->grp ? s->grpDt + (size_t)slot * s->nGrp : s->dtDev + slot;
+}
+
 StageArgs base_args(frg_solver *s) {
   StageArgs a{};
   a.nE = s->L;
@@ -339,7 +365,8 @@ StageArgs base_args(frg_solver *s) {
   a.JG = s->JG;
   a.detJ = s->detJs;
   a.waveSp = s->waveSp;
-  a.dt = s->p.dtType == 2 ? s->eleDt : s->dtDev + s->dtCur;
+  a.dt = s->p.dtType == 2 ? s->eleDt : dt_slot(s, s->dtCur);
+  a.grp = s->grp;
   a.dtLocal = s->p.dtType == 2;
   a.time = s->timeDev;
   a.err = s->err;
@@ -354,7 +381,7 @@ StageArgs base_args(frg_solver *s) {
   a.dAd = s->dAd;
   a.wsurf = s->wsurf;
   a.blockMin = s->blockMin;
-  a.dtNext = s->dtDev + (s->dtCur ^ 1);
+  a.dtNext = dt_slot(s, s->dtCur ^ 1);
   a.eleDt = s->eleDt;
   a.ticket = s->ticket;
   a.cflFac = s->p.CFL * kCflLimit[s->p.order] * 2;
@@ -430,8 +457,9 @@ frg_status launch_stage_args(frg_solver *s, StageArgs &a) {
 frg_status launch_dt(frg_solver *s) {
   int nb = (s->nE + 31) / 32;
   double fac = s->p.CFL * kCflLimit[s->p.order] * 2;
+  if (s->grp) CK(cudaMemsetAsync(dt_slot(s, s->dtCur), 0x7F, (size_t)s->nGrp * 8, s->stream));
   fr_dt_kernel<<<nb, 256, 0, s->stream>>>(s->waveSp, s->dAd, s->vol, s->wsurf, s->nF, s->g.nFF, s->nE, s->L, fac,
-                                           s->eleDt, s->blockMin, s->ticket, s->dtDev + s->dtCur, s->err);
+                                           s->eleDt, s->blockMin, s->ticket, dt_slot(s, s->dtCur), s->err, s->grp);
   s->dtLast = s->dtCur;
   return post_launch(s);
 }
@@ -452,6 +480,12 @@ void drop_graphs(frg_solver *s) {
 // The last stage of the TMA kernel computes the next step's global CFL dt.
 bool fused_dt(const frg_solver *s) { return s->useTma && s->p.dtType == 1; }
 
+frg_status launch_group_step(frg_solver *s) {
+  fr_group_step_kernel<<<(s->nGrp + 127) / 128, 128, 0, s->stream>>>(
+      dt_slot(s, s->dtCur), fused_dt(s) ? dt_slot(s, s->dtCur ^ 1) : nullptr, s->grpTime, s->nGrp);
+  return post_launch(s);
+}
+
 // dt work at the start of the next fused step (see frg_solver::graph).
 int dt_mode(const frg_solver *s) {
   if (s->p.dtType == 0) return 0;
@@ -469,9 +503,10 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
   if (s->p.dtType != 0) {
     if (mode == 2 && (st = launch_wavesp(s))) return st;
     if (mode >= 1 && (st = launch_dt(s))) return st;
-    if (fused_dt(s))  // the slot the last stage will minimise into
+    if (fused_dt(s) && !s->grp)  // the slot the last stage will minimise into
       CK(cudaMemsetAsync(s->dtDev + (s->dtCur ^ 1), 0x7F, sizeof(double), s->stream));
   }
+  if (s->grp && (st = launch_group_step(s))) return st;
   if (ev) CK(cudaEventRecord(ev[1], s->stream));
   const int nRK = s->nRK;
   const bool jam = s->p.timeType == 5;
@@ -693,7 +728,9 @@ frg_status frg_destroy(frg_solver *s) {
                   s->nrmOwn, s->dAd, s->vol, s->wsurf, s->wvol, s->waveSp, s->eleDt, s->dtDev, s->timeDev,
                   s->blockMin, s->normPartial, s->normOut, s->scratchRef};
   for (double *q : dp) if (q) cudaFree(q);
-  void *vp[] = {s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->invDetS, s->nbr, s->err,
+  cudaFree(s->grpDt);
+  cudaFree(s->grpTime);
+  void *vp[] = {s->grp, s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->invDetS, s->nbr, s->err,
                 s->ticket,
                 s->fvn, s->fvn2};
   for (void *q : vp) if (q) cudaFree(q);
@@ -906,6 +943,7 @@ frg_status frg_calc_residual(frg_solver *s, int step) {
 
 frg_status frg_time_step_a(frg_solver *s, int step, double rkval) {
   if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
+  if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: advance with frg_update");
   const long n = (long)s->nV * s->nS * s->L;
   fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
       s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev + s->dtCur, s->p.dtType == 2, rkval, 0,
@@ -916,6 +954,7 @@ frg_status frg_time_step_a(frg_solver *s, int step, double rkval) {
 
 frg_status frg_time_step_b(frg_solver *s, int step) {
   if (!s || step < 0 || step >= s->nRK || !s->divF[step]) return fail(FRG_ERR_ARG, "bad step / residual missing");
+  if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: advance with frg_update");
   const long n = (long)s->nV * s->nS * s->L;
   fr_timestep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
       s->U, s->U0, s->divF[step], s->detJd, s->p.dtType == 2 ? s->eleDt : s->dtDev + s->dtCur, s->p.dtType == 2,
@@ -938,6 +977,7 @@ frg_status frg_copy_u0_to_u(frg_solver *s) {
 
 frg_status frg_calc_dt(frg_solver *s, double *dt_out) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
+  if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: per-group dt via frg_update / frg_get_group_times");
   frg_status st;
   if (s->p.dtType != 0) {
     if (s->iter == s->initIter + 1) {
@@ -958,6 +998,7 @@ frg_status frg_update(frg_solver *s, int nsteps) {
   if (!s || nsteps < 0) return fail(FRG_ERR_ARG, "bad arguments");
   frg_status st;
   if (s->p.timeType == 0 && s->p.dtType != 0) {
+    if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: Forward Euler with CFL dt is not supported");
     // Forward Euler takes its CFL dt after the residual (src/solver.cpp:238-241):
     // the reference's unfused sequence
     for (int n = 0; n < nsteps; n++)
@@ -985,7 +1026,7 @@ frg_status frg_update(frg_solver *s, int nsteps) {
     }
     CK(cudaGraphLaunch(ge, s->stream));
     // count the kernels the graph holds
-    s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? mode : 0);
+    s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? mode : 0) + (s->grp ? 1 : 0);
     s->curTr ^= (s->nRK & 1);
     s->dtFresh = fused_dt(s);
     s->dtLast = s->dtCur;
@@ -1032,8 +1073,10 @@ frg_status frg_set_monitor(frg_solver *s, int enable) {
 
 frg_status frg_get_time(const frg_solver *s, double *time, double *dt, int *iter) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
-  if (time) { CK(cudaMemcpyAsync(time, s->timeDev, 8, cudaMemcpyDeviceToHost, s->stream)); }
-  if (dt) { CK(cudaMemcpyAsync(dt, s->dtDev + s->dtLast, 8, cudaMemcpyDeviceToHost, s->stream)); }
+  // (ensemble mode: group 0's; all groups through frg_get_group_times)
+  const double *tsrc = s->grp ? s->grpTime : s->timeDev;
+  if (time) { CK(cudaMemcpyAsync(time, tsrc, 8, cudaMemcpyDeviceToHost, s->stream)); }
+  if (dt) { CK(cudaMemcpyAsync(dt, dt_slot(const_cast<frg_solver *>(s), s->dtLast), 8, cudaMemcpyDeviceToHost, s->stream)); }
   CK(cudaStreamSynchronize(s->stream));
   if (iter) *iter = s->iter;
   return FRG_OK;
@@ -1071,6 +1114,42 @@ frg_status frg_set_tile_variant(frg_solver *s, int variant) {
   return setup_tma(s);
 }
 
+frg_status frg_set_groups(frg_solver *s, const int *groupOfElement, int nGroups, const double *fixedDt) {
+  if (!s || !groupOfElement || nGroups < 1) return fail(FRG_ERR_ARG, "bad arguments");
+  if (s->p.dtType == 2) return fail(FRG_ERR_ARG, "ensemble mode: local dt (dtType 2) not supported");
+  if (s->p.dtType == 0 && !fixedDt) return fail(FRG_ERR_ARG, "ensemble mode with dtType 0 needs one dt per group");
+  std::vector<int> g((size_t)s->L, 0);
+  for (int e = 0; e < s->nE; e++) {
+    g[e] = groupOfElement[e];
+    if (g[e] < 0 || g[e] >= nGroups) return fail(FRG_ERR_ARG, "element %d: group %d out of range", e, g[e]);
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  drop_graphs(s);
+  cudaFree(s->grp);
+  cudaFree(s->grpDt);
+  cudaFree(s->grpTime);
+  s->grp = nullptr;
+  s->grpDt = s->grpTime = nullptr;
+  frg_status st;
+  if ((st = dalloc(&s->grp, g.size())) || (st = dalloc(&s->grpDt, 2 * (size_t)nGroups)) ||
+      (st = dalloc(&s->grpTime, nGroups)))
+    return st;
+  CK(cudaMemcpy(s->grp, g.data(), g.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (fixedDt) CK(cudaMemcpy(s->grpDt, fixedDt, (size_t)nGroups * 8, cudaMemcpyHostToDevice));
+  s->nGrp = nGroups;
+  s->dtCur = s->dtLast = 0;
+  s->dtFresh = false;
+  return FRG_OK;
+}
+
+frg_status frg_get_group_times(frg_solver *s, double *time, double *dt) {
+  if (!s || !s->grp) return fail(FRG_ERR_ARG, "no groups set (frg_set_groups)");
+  if (time) CK(cudaMemcpyAsync(time, s->grpTime, (size_t)s->nGrp * 8, cudaMemcpyDeviceToHost, s->stream));
+  if (dt) CK(cudaMemcpyAsync(dt, dt_slot(s, s->dtLast), (size_t)s->nGrp * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FRG_OK;
+}
+
 frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out) {
   if (!s || nsteps < 1) return fail(FRG_ERR_ARG, "bad arguments");
   const int nVar = s->useTma ? s->ks.nTma : 1;
@@ -1078,9 +1157,10 @@ frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_
     // the trial steps advance the solution: keep everything they change
     const size_t nU = (size_t)s->nV * s->nS * s->L, nW = (size_t)s->nF * s->L, nD = (size_t)s->L;
     double *save = nullptr;
-    frg_status st = dalloc(&save, 2 * nU + nW + nD + 3);
+    const size_t nG = s->grp ? 3 * (size_t)s->nGrp : 0;
+    frg_status st = dalloc(&save, 2 * nU + nW + nD + 3 + nG);
     if (st) return st;
-    double *sU = save, *sD0 = save + nU, *sWs = save + 2 * nU, *sEd = sWs + nW, *sDt = sEd + nD;
+    double *sU = save, *sD0 = save + nU, *sWs = save + 2 * nU, *sEd = sWs + nW, *sDt = sEd + nD, *sG = sDt + 3;
     const bool hadDiv = s->divF0Valid && s->divF[0];
     auto cp = [&](double *dst, const double *src, size_t n) {
       return cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToDevice, s->stream);
@@ -1091,6 +1171,10 @@ frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_
     CK(cp(sEd, s->eleDt, nD));
     CK(cp(sDt, s->dtDev, 2));
     CK(cp(sDt + 2, s->timeDev, 1));
+    if (nG) {
+      CK(cp(sG, s->grpDt, 2 * (size_t)s->nGrp));
+      CK(cp(sG + 2 * (size_t)s->nGrp, s->grpTime, s->nGrp));
+    }
     const int iter = s->iter, dtCur = s->dtCur, dtLast = s->dtLast, curTr = s->curTr;
     const bool dtFresh = s->dtFresh, divValid = s->divF0Valid;
     cudaEvent_t e0, e1;
@@ -1131,6 +1215,10 @@ frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_
     CK(cp(s->eleDt, sEd, nD));
     CK(cp(s->dtDev, sDt, 2));
     CK(cp(s->timeDev, sDt + 2, 1));
+    if (nG) {
+      CK(cp(s->grpDt, sG, 2 * (size_t)s->nGrp));
+      CK(cp(s->grpTime, sG + 2 * (size_t)s->nGrp, s->nGrp));
+    }
     CK(cudaStreamSynchronize(s->stream));
     cudaFree(save);
     s->iter = iter;
@@ -1270,11 +1358,12 @@ namespace {
 // Seed of the last RK stage from the adjoint of a step's final state:
 // gbar = -b_last * dt / detJ * lam.
 __global__ void fr_adj_seed_kernel(const double *lam, const double *detJ, double *seed, double coef, int NV, int NS,
-                                   int nE, int L) {
+                                   int nE, int L, const int *grp, const double *dtGrp) {
   const long n = (long)NV * NS * L;
   for (long it = blockIdx.x * (long)blockDim.x + threadIdx.x; it < n; it += (long)gridDim.x * blockDim.x) {
     const int e = (int)(it % L), s = (int)((it / L) % NS);
-    seed[it] = e < nE ? coef * lam[it] / detJ[(size_t)s * L + e] : 0.0;
+    const double c = grp ? coef * dtGrp[grp[e]] : coef;
+    seed[it] = e < nE ? c * lam[it] / detJ[(size_t)s * L + e] : 0.0;
   }
 }
 
@@ -1326,6 +1415,8 @@ AdjArgs adj_args(frg_solver *s, const double *Y, const double *gbar) {
   a.err = s->err;
   a.thetaBar = s->adj->thetaBar;
   a.thetaDir = s->adj->thetaDir;
+  a.grp = s->grp;
+  a.dtGrp = s->grpDt;  // slot 0: the fixed per-group dt
   a.ph = make_phys(s->p);
   return a;
 }
@@ -1414,6 +1505,7 @@ frg_status step_keep_stages(frg_solver *s, double *const *Y, bool advanceTime = 
     a.bCur = s->RKb[k];
     a.flags = (last ? SF_LAST : 0) | (first ? SF_FIRST : 0) | (last && advanceTime ? SF_TIME : 0);
     a.Acc = s->Acc;
+    if (first && advanceTime && s->grp && (st = launch_group_step(s))) return st;
     if (s->useTma) {
       a.Uin_d = first ? s->U : nullptr;
       a.Uin_s = first ? nullptr : Y[k];
@@ -1572,8 +1664,10 @@ frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const do
   CK(cudaMemcpy(ad->thetaDir, thetaDir ? thetaDir : zero, 5 * 8, cudaMemcpyHostToDevice));
   const double dt = s->p.dt;  // fixed dt (dtType 0)
   const int nb = (int)std::min<size_t>((nSE + 255) / 256, 148 * 8);
-  fr_adj_seed_kernel<<<nb, 256, 0, s->stream>>>(ad->lam[0], s->detJd, ad->seed[0], -s->RKb[nRK - 1] * dt, s->nV,
-                                                 s->nS, s->nE, s->L);
+  // (ensemble mode: the per-group fixed dt multiplies per element)
+  fr_adj_seed_kernel<<<nb, 256, 0, s->stream>>>(ad->lam[0], s->detJd, ad->seed[0],
+                                                 -s->RKb[nRK - 1] * (s->grp ? 1.0 : dt), s->nV, s->nS, s->nE, s->L,
+                                                 s->grp, s->grpDt);
   if ((st = post_launch(s))) return st;
   int cl = 0, cs = 0;  // current lam / seed buffers
   double *seg = ad->stages;

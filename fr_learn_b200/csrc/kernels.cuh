@@ -162,7 +162,8 @@ struct StageArgs {
   const void *JG;       // (S) [DIM][DIM][NS][nE]
   const void *detJ;     // (S) [NS][nE]
   double *waveSp;       // [NF][nE]
-  const double *dt;     // scalar, or [nE] when dtLocal
+  const double *dt;     // scalar, [nE] when dtLocal, or one per group when grp is set
+  const int *grp;       // ensemble mode: group (independent case) of each element, else null
   double *time;         // device time (SF_TIME)
   unsigned *err;
   double aNext, bCur;
@@ -267,7 +268,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
   S *Wout = static_cast<S *>(a.Wout);
   const int nE = a.nE;
   const bool resid = a.flags & SF_RESIDUAL;
-  const double dtG = (resid || a.dtLocal) ? 0.0 : __ldg(a.dt);
+  const double dtG = (resid || a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
     if (eg >= a.nEle) continue;
@@ -278,7 +279,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
     double det = 0, dtl = 0;
     if (!resid) {
       det = (double)detJG[(size_t)s * nE + eg];
-      dtl = a.dtLocal ? a.dt[eg] : dtG;
+      dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
     }
 #pragma unroll
     for (int v = 0; v < NV; v++) {
@@ -322,7 +323,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
       Us[(v * NS + s) * TE + e] = (R)(last ? unew : (double)(S)unew);
     }
   }
-  if (!resid && (a.flags & SF_TIME) && blockIdx.x == 0 && threadIdx.x == 0) *a.time += a.dt[0];
+  if (!resid && !a.grp && (a.flags & SF_TIME) && blockIdx.x == 0 && threadIdx.x == 0) *a.time += a.dt[0];
 }
 
 // Phase D: traces of the new state for the next launch.

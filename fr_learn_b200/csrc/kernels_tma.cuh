@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
   }
 
   // the global dt, fetched while the tiles are in flight
-  const double dtG = a.dtLocal ? 0.0 : __ldg(a.dt);
+  const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
 
   // ---- group 0: gathers of neighbour traces, then phase A
   bool ok = mbar_wait(&bar[0], 0);
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
     int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
     corr_fpts<C>(i, j, k, cf, cs, ca);
     const double idet = (double)sDet[s * TE + e];  // 1 / detJ
-    const double dtl = a.dtLocal ? a.dt[eg] : dtG;
+    const double dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
 #pragma unroll
     for (int v = 0; v < NV; v++) {
       R acc = 0;
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
       Us[o] = (R)(last ? unew : (double)(S)unew);
     }
   }
-  if ((flags & SF_TIME) && blockIdx.x == 0 && tid == 0) *a.time += dtG;
+  if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
@@ -381,12 +381,17 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
         const double dte = a.cflFac * a.vol[eg] / iw;
         a.eleDt[eg] = dte;
         my = dte;
+        if (a.grp) {  // ensemble mode: each element into its own group's minimum
+          if (!(dte > 1e-13)) atomicOr(a.err, ERRF_DT);
+          else atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext + a.grp[eg]),
+                         (unsigned long long)__double_as_longlong(dte));
+        }
       }
       for (int o = 16; o > 0; o >>= 1) {
         const double t = __shfl_xor_sync(0xffffffffu, my, o);
         my = (isnan(t) || t < my) ? t : my;
       }
-      if (tid == 0) {
+      if (tid == 0 && !a.grp) {
         if (!(my > 1e-13)) atomicOr(a.err, ERRF_DT);  // also catches NaN
         else atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext), (unsigned long long)__double_as_longlong(my));
       }

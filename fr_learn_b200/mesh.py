@@ -246,3 +246,25 @@ def bump2d(nx=96, ny=32, x0=-1.5, x1=1.5, height=0.8, amp=0.0625, width=25.0, cl
             e += 1
     verts = np.stack([PX.ravel(), PY.ravel()], axis=-1)
     return Mesh(2, xv, c2v, bc, verts=verts, name=f"bump2d_{nx}x{ny}")
+
+
+def concat_meshes(meshes):
+    """One mesh holding independent cases side by side (for the ensemble
+    mode): element arrays stacked, vertex ids offset per case so no face joins
+    two cases.  Returns (mesh, group of each element)."""
+    assert meshes and all(m.nDims == meshes[0].nDims and m.nNodes == meshes[0].nNodes for m in meshes)
+    xv, c2v, bc, verts, grp = [], [], [], [], []
+    off = 0
+    for g, m in enumerate(meshes):
+        nv = int(m.c2v.max()) + 1 if m.verts is None else len(m.verts)
+        xv.append(m.xv)
+        c2v.append(m.c2v + off)
+        bc.append(m.bc)
+        if m.verts is not None:
+            verts.append(m.verts)
+        grp.append(np.full(m.nEles, g, np.int32))
+        off += nv
+    out = Mesh(meshes[0].nDims, np.concatenate(xv), np.concatenate(c2v).astype(np.int32), np.concatenate(bc),
+               verts=np.concatenate(verts) if len(verts) == len(meshes) else None,
+               name=f"ensemble_{len(meshes)}")
+    return out, np.concatenate(grp)

@@ -102,6 +102,8 @@ def lib():
         "frg_autotune": ([vp, i, C.POINTER(C.c_int), vp], i),
         "frg_set_tile_variant": ([vp, i], i),
         "frg_objective": ([vp, i, C.POINTER(d), vp], i),
+        "frg_set_groups": ([vp, vp, i, vp], i),
+        "frg_get_group_times": ([vp, vp, vp], i),
         "frg_residual_vjp": ([vp, vp, vp, vp, C.POINTER(d)], i),
         "frg_adjoint_forward": ([vp, i, i], i),
         "frg_adjoint_backward": ([vp, vp, vp, vp, C.POINTER(d)], i),
@@ -268,6 +270,28 @@ class Solver:
         out = np.zeros(4)
         _check(lib().frg_autotune(self.h, nsteps, C.byref(v), out.ctypes.data))
         return v.value, out
+
+    # -- ensemble mode
+    def set_groups(self, group_of_element, n_groups, fixed_dt=None):
+        """Independent cases in one mesh: per-group CFL dt (or fixed_dt[g])
+        and time; see frg_set_groups."""
+        g = np.ascontiguousarray(group_of_element, np.int32)
+        assert g.shape == (self.nEles,)
+        self._groups = g
+        fd = None
+        if fixed_dt is not None:
+            fd = np.ascontiguousarray(fixed_dt, np.float64)
+            assert fd.shape == (n_groups,)
+        self._fixed_dt = fd
+        self.n_groups = n_groups
+        _check(lib().frg_set_groups(self.h, g.ctypes.data, n_groups, None if fd is None else fd.ctypes.data))
+
+    def group_times(self):
+        """(time per group, dt of the last step per group)."""
+        t = np.empty(self.n_groups)
+        dt = np.empty(self.n_groups)
+        _check(lib().frg_get_group_times(self.h, t.ctypes.data, dt.ctypes.data))
+        return t, dt
 
     # -- discrete adjoint (FP64, inviscid, fixed dt)
     OBJECTIVES = {"entropy": 1, "wall_pressure": 2}

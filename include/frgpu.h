@@ -207,6 +207,19 @@ frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long
 frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out);
 /* Selects a tile shape of the TMA stage kernel by index (0 = default). */
 frg_status frg_set_tile_variant(frg_solver *s, int variant);
+/* ---- Ensemble mode (no counterpart in the reference) ---------------------
+ * Many independent cases of one order in one handle: the mesh is the union
+ * of the cases' meshes (no face joins two cases) and groupOfElement gives
+ * each element's case.  Each case keeps its own CFL dt (the minimum over its
+ * own elements, dtType 1) or the fixed dt given per case (dtType 0,
+ * fixedDt[nGroups]), and its own time; everything else is shared, so one
+ * launch per RK stage advances every case.  frg_calc_dt / frg_time_step_a/b
+ * are not available in this mode (frg_update only); frg_get_time reports
+ * group 0. */
+frg_status frg_set_groups(frg_solver *s, const int *groupOfElement, int nGroups, const double *fixedDt);
+/* Per-group time and the dt of the last step (nGroups doubles each). */
+frg_status frg_get_group_times(frg_solver *s, double *time, double *dt);
+
 /* ---- Discrete adjoint (no counterpart in the reference) ----------------
  * FP64, inviscid (Euler or advection), fixed dt (dtType 0), RK tables of
  * timeType 0/2/4.  The adjoint kernels transpose the residual operation by
