@@ -238,6 +238,8 @@ struct frg_solver {
   // step's last stage already computed dt, 1 = dt kernel first, 2 = wave
   // speeds + dt first
   cudaGraphExec_t graph[3][2][2] = {};
+  cudaGraph_t graphRaw[3][2][2] = {};  // the captured graphs (child nodes of an ensemble step)
+  unsigned graphEpoch = 0;             // bumped whenever the captured graphs are dropped
   bool dtFresh = false;  // device dt was computed from the current wave speeds
   // tensor maps of the TMA stage kernel
   bool useTma = false;
@@ -475,6 +477,11 @@ void drop_graphs(frg_solver *s) {
     for (auto &q : r)
       for (auto &g : q)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto &r : s->graphRaw)
+    for (auto &q : r)
+      for (auto &g : q)
+        if (g) { cudaGraphDestroy(g); g = nullptr; }
+  s->graphEpoch++;
 }
 
 // The last stage of the TMA kernel computes the next step's global CFL dt.
@@ -994,6 +1001,38 @@ frg_status frg_calc_dt(frg_solver *s, double *dt_out) {
   return FRG_OK;
 }
 
+// The captured graph of one fused step in the solver's current state
+// (dt mode, trace buffer, dt slot), captured on first use.
+static frg_status step_graph(frg_solver *s, int mode, cudaGraphExec_t *exec, cudaGraph_t *raw) {
+  const int ct = s->curTr;
+  cudaGraphExec_t &ge = s->graph[mode][ct][s->dtCur];
+  cudaGraph_t &gr = s->graphRaw[mode][ct][s->dtCur];
+  if (!ge) {
+    const long long before = s->launches;
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    frg_status st = enqueue_step(s, mode);
+    cudaError_t ce = cudaStreamEndCapture(s->stream, &gr);
+    if (st) return st;
+    if (ce != cudaSuccess) return fail(FRG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    CK(cudaGraphInstantiate(&ge, gr, 0));
+    s->launches = before;
+    s->curTr = ct;
+  }
+  if (exec) *exec = ge;
+  if (raw) *raw = gr;
+  return FRG_OK;
+}
+
+// Host bookkeeping after a captured step was launched.
+static void step_done(frg_solver *s, int mode) {
+  // count the kernels the graph holds
+  s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? mode : 0) + (s->grp ? 1 : 0);
+  s->curTr ^= (s->nRK & 1);
+  s->dtFresh = fused_dt(s);
+  s->dtLast = s->dtCur;
+  s->dtCur ^= (int)s->dtFresh;
+}
+
 frg_status frg_update(frg_solver *s, int nsteps) {
   if (!s || nsteps < 0) return fail(FRG_ERR_ARG, "bad arguments");
   frg_status st;
@@ -1009,28 +1048,10 @@ frg_status frg_update(frg_solver *s, int nsteps) {
   for (int n = 0; n < nsteps; n++) {
     s->iter++;
     const int mode = dt_mode(s);
-    const int ct = s->curTr;
-    cudaGraphExec_t &ge = s->graph[mode][ct][s->dtCur];
-    if (!ge) {
-      cudaGraph_t gr;
-      long long before = s->launches;
-      CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-      st = enqueue_step(s, mode);
-      cudaError_t ce = cudaStreamEndCapture(s->stream, &gr);
-      if (st) return st;
-      if (ce != cudaSuccess) return fail(FRG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-      CK(cudaGraphInstantiate(&ge, gr, 0));
-      CK(cudaGraphDestroy(gr));
-      s->launches = before;
-      s->curTr = ct;
-    }
+    cudaGraphExec_t ge;
+    if ((st = step_graph(s, mode, &ge, nullptr))) return st;
     CK(cudaGraphLaunch(ge, s->stream));
-    // count the kernels the graph holds
-    s->launches += s->nRK * (s->ks.grad ? 2 : 1) + (s->p.dtType != 0 ? mode : 0) + (s->grp ? 1 : 0);
-    s->curTr ^= (s->nRK & 1);
-    s->dtFresh = fused_dt(s);
-    s->dtLast = s->dtCur;
-    s->dtCur ^= (int)s->dtFresh;
+    step_done(s, mode);
   }
   if (nsteps > 0) s->divF0Valid = s->monitor;
   return check_flags(s);
@@ -1729,6 +1750,104 @@ frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const do
   if (lam0_host && (st = state_to_host(s, ad->lam[cl], lam0_host))) return st;
   CK(cudaStreamSynchronize(s->stream));
   return check_flags(s);
+}
+
+}  // extern "C"
+
+// ==================================================================== ensemble
+// Several handles (one per order of a batch of cases) advanced together: each
+// step is ONE graph launch whose parallel branches are the handles' own
+// captured steps (child graphs), so the orders' kernels share the GPU.
+
+struct frg_ensemble {
+  std::vector<frg_solver *> ss;
+  cudaStream_t stream = nullptr, ownStream = nullptr;
+  std::map<std::vector<int>, cudaGraphExec_t> graphs;  // per combination of the handles' step keys
+  std::vector<unsigned> epochs;                        // the handles' graph epochs the graphs were built at
+};
+
+extern "C" {
+
+frg_status frg_ensemble_create(frg_solver *const *solvers, int n, frg_ensemble **out) {
+  if (!solvers || n < 1 || !out) return fail(FRG_ERR_ARG, "bad arguments");
+  for (int i = 0; i < n; i++) {
+    if (!solvers[i]) return fail(FRG_ERR_ARG, "null handle %d", i);
+    if (solvers[i]->p.timeType == 0 && solvers[i]->p.dtType != 0)
+      return fail(FRG_ERR_ARG, "handle %d: Forward Euler with CFL dt is not fused", i);
+  }
+  std::unique_ptr<frg_ensemble> e(new frg_ensemble);
+  e->ss.assign(solvers, solvers + n);
+  CK(cudaStreamCreateWithFlags(&e->ownStream, cudaStreamNonBlocking));
+  e->stream = e->ownStream;
+  *out = e.release();
+  return FRG_OK;
+}
+
+frg_status frg_ensemble_set_stream(frg_ensemble *e, void *stream) {
+  if (!e) return fail(FRG_ERR_ARG, "null ensemble");
+  CK(cudaStreamSynchronize(e->stream));
+  e->stream = stream ? (cudaStream_t)stream : e->ownStream;
+  return FRG_OK;
+}
+
+frg_status frg_ensemble_update(frg_ensemble *e, int nsteps) {
+  if (!e || nsteps < 0) return fail(FRG_ERR_ARG, "bad arguments");
+  frg_status st;
+  std::vector<unsigned> ep;
+  for (frg_solver *s : e->ss) {
+    if ((st = ensure_traces(s))) return st;
+    CK(cudaStreamSynchronize(s->stream));
+    ep.push_back(s->graphEpoch);
+  }
+  if (ep != e->epochs) {  // a handle re-captured its steps: rebuild
+    for (auto &g : e->graphs) cudaGraphExecDestroy(g.second);
+    e->graphs.clear();
+    e->epochs = ep;
+  }
+  const size_t n = e->ss.size();
+  std::vector<int> key(3 * n), mode(n);
+  for (int step = 0; step < nsteps; step++) {
+    for (size_t i = 0; i < n; i++) {
+      frg_solver *s = e->ss[i];
+      s->iter++;
+      mode[i] = dt_mode(s);
+      key[3 * i] = mode[i];
+      key[3 * i + 1] = s->curTr;
+      key[3 * i + 2] = s->dtCur;
+    }
+    auto it = e->graphs.find(key);
+    if (it == e->graphs.end()) {
+      cudaGraph_t g;
+      CK(cudaGraphCreate(&g, 0));
+      for (size_t i = 0; i < n; i++) {
+        cudaGraph_t raw;
+        if ((st = step_graph(e->ss[i], mode[i], nullptr, &raw))) return st;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddChildGraphNode(&node, g, nullptr, 0, raw));
+      }
+      cudaGraphExec_t ex;
+      CK(cudaGraphInstantiate(&ex, g, 0));
+      CK(cudaGraphDestroy(g));
+      it = e->graphs.emplace(key, ex).first;
+    }
+    CK(cudaGraphLaunch(it->second, e->stream));
+    for (size_t i = 0; i < n; i++) step_done(e->ss[i], mode[i]);
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  for (frg_solver *s : e->ss) {
+    if (nsteps > 0) s->divF0Valid = s->monitor;
+    if ((st = check_flags(s))) return st;
+  }
+  return FRG_OK;
+}
+
+frg_status frg_ensemble_destroy(frg_ensemble *e) {
+  if (!e) return FRG_OK;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (auto &g : e->graphs) cudaGraphExecDestroy(g.second);
+  if (e->ownStream) cudaStreamDestroy(e->ownStream);
+  delete e;
+  return FRG_OK;
 }
 
 }  // extern "C"

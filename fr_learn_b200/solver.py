@@ -103,6 +103,10 @@ def lib():
         "frg_set_tile_variant": ([vp, i], i),
         "frg_objective": ([vp, i, C.POINTER(d), vp], i),
         "frg_set_groups": ([vp, vp, i, vp], i),
+        "frg_ensemble_create": ([vp, i, C.POINTER(vp)], i),
+        "frg_ensemble_set_stream": ([vp, vp], i),
+        "frg_ensemble_update": ([vp, i], i),
+        "frg_ensemble_destroy": ([vp], i),
         "frg_get_group_times": ([vp, vp, vp], i),
         "frg_residual_vjp": ([vp, vp, vp, vp, C.POINTER(d)], i),
         "frg_adjoint_forward": ([vp, i, i], i),
@@ -371,3 +375,31 @@ def inspect_geometry(mesh: Mesh, which: str, **params) -> np.ndarray:
     if which == "faces":
         return out.reshape(-1, 6).astype(np.int64)
     return out
+
+
+class Ensemble:
+    """Solvers advanced together, one graph launch per step (frg_ensemble)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s.h for s in self.solvers])
+        h = C.c_void_p()
+        _check(lib().frg_ensemble_create(arr, len(self.solvers), C.byref(h)))
+        self.h = h
+
+    def set_stream(self, stream_ptr):
+        _check(lib().frg_ensemble_set_stream(self.h, stream_ptr))
+
+    def update(self, nsteps=1):
+        _check(lib().frg_ensemble_update(self.h, nsteps))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().frg_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -220,6 +220,16 @@ frg_status frg_set_groups(frg_solver *s, const int *groupOfElement, int nGroups,
 /* Per-group time and the dt of the last step (nGroups doubles each). */
 frg_status frg_get_group_times(frg_solver *s, double *time, double *dt);
 
+/* Handles advanced together, e.g. one per order of a batch of cases: each
+ * step is one CUDA graph launch whose parallel branches are the handles' own
+ * captured fused steps.  frg_ensemble_update returns after the steps
+ * finished and each handle's error flags were checked. */
+typedef struct frg_ensemble frg_ensemble;
+frg_status frg_ensemble_create(frg_solver *const *solvers, int n, frg_ensemble **out);
+frg_status frg_ensemble_set_stream(frg_ensemble *e, void *stream);
+frg_status frg_ensemble_update(frg_ensemble *e, int nsteps);
+frg_status frg_ensemble_destroy(frg_ensemble *e);
+
 /* ---- Discrete adjoint (no counterpart in the reference) ----------------
  * FP64, inviscid (Euler or advection), fixed dt (dtType 0), RK tables of
  * timeType 0/2/4.  The adjoint kernels transpose the residual operation by

@@ -88,3 +88,35 @@ def test_ensemble_adjoint_matches_cases_alone():
     lam_e = e.adjoint_backward()[0]
     for k in range(3):
         assert relerr(lam_e[:, grp == k], lam[k]) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cross_order_ensemble_graph_matches_separate_updates(precision):
+    """Two order groups (P=2, P=4), each the union of two cases, stepped by one
+    graph launch per step give what each group's own frg_update gives."""
+    from fr_learn_b200 import Ensemble, Solver, concat_meshes
+
+    cases = _cases()
+    outs = []
+    for use_ens in (False, True):
+        solvers = []
+        for P, idx in ((2, (0, 1)), (4, (1, 2))):
+            union, grp = concat_meshes([cases[i] for i in idx])
+            s = Solver(union, order=P, riemannType=1, dtType=1, CFL=0.5, precision=precision)
+            s.set_groups(grp, 2)
+            pos = s.get("pos_spts")
+            s.set("U_spts", np.concatenate([_vortex(pos[:, grp == k], 2.0 + k, (0.5, -0.3)) for k in range(2)],
+                                           axis=1))
+            solvers.append(s)
+        if use_ens:
+            ens = Ensemble(solvers)
+            ens.update(3)
+            ens.update(4)
+            ens.close()
+        else:
+            for s in solvers:
+                s.update(7)
+        outs.append([(s.get("U_spts"), s.group_times()) for s in solvers])
+    for (Ua, (ta, da)), (Ub, (tb, db)) in zip(outs[0], outs[1]):
+        assert np.array_equal(Ua, Ub)
+        assert np.array_equal(ta, tb) and np.array_equal(da, db)
