@@ -237,6 +237,7 @@ def run_gpu(args, rank, world, local_rank):
     for sv in solvers.values():
         sv.set_stream(None)
     res["adjoint"] = run_adjoint_bump(stream)
+    res["ensemble"] = run_ensemble(stream)
     return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
 
 
@@ -318,6 +319,134 @@ def run_adjoint_bump(stream, nsteps=500, every=25):
                                                                       / np.abs(lam0).max())},
             "J_wall_pressure": J, "dJ_dMach": dJdM, "dJ_dMach_central_difference": fd,
             "dJ_dMach_rel_diff": abs(dJdM - fd) / abs(fd)}
+
+
+def ensemble_cases(n=256, seed=2024):
+    """The batched workload: n independent 2D Euler isentropic-vortex cases on
+    periodic [-10,10]^2 squares of side x side perturbed quads, side uniform
+    in {16,24,...,96}, order P uniform in {2,3,4,5}, vortex strength uniform
+    in [1,5], freestream Mach uniform in [0.1,0.6] along (1,1) (rho = p = 1),
+    all drawn from one seeded generator."""
+    rng = np.random.default_rng(seed)
+    sides = np.arange(16, 97, 8)
+    out = []
+    for c in range(n):
+        out.append(dict(side=int(rng.choice(sides)), P=int(rng.integers(2, 6)), eps=float(rng.uniform(1, 5)),
+                        mach=float(rng.uniform(0.1, 0.6)), seed=c))
+    return out
+
+
+def vortex_state(pos, eps, mach, gamma=1.4):
+    """Isentropic vortex of strength eps centred at the origin in a freestream
+    of Mach `mach` along (1,1), rho = p = 1 (the vortex of ele::setInitialCondition,
+    src/ele.cpp:708-733, with the strength and freestream as parameters)."""
+    ui = mach * np.sqrt(gamma) / np.sqrt(2.0)
+    x, y = pos[..., 0], pos[..., 1]
+    f = 1.0 - (x * x + y * y)
+    rho = (1.0 - eps * eps * (gamma - 1.0) / (8.0 * gamma * np.pi ** 2) * np.exp(f)) ** (1.0 / (gamma - 1.0))
+    u = ui - eps * y / (2 * np.pi) * np.exp(f / 2)
+    v = ui + eps * x / (2 * np.pi) * np.exp(f / 2)
+    p = rho ** gamma
+    return np.stack([rho, rho * u, rho * v, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)], axis=-1)
+
+
+def run_ensemble(stream, nsteps=500, warmup=3, alone_steps=20, adj_steps=100):
+    """Batched ensemble: the 256 cases grouped by order, each group one handle
+    in ensemble mode (per-case CFL dt), the four handles advanced by one graph
+    launch per step; against the same cases run one by one.  Then the adjoint
+    of each case's final entropy error (FP64, per-case dt frozen at the first
+    step's CFL value), per order group."""
+    import torch
+
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Ensemble, Solver, box2d, concat_meshes
+
+    cases = ensemble_cases()
+    kw = dict(riemannType=1, timeType=4, CFL=0.5, gamma=1.4)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+        return a.elapsed_time(b)
+
+    meshes = {c["seed"]: box2d(c["side"], c["side"], -10, 10, -10, 10, perturb=0.1, seed=c["seed"]) for c in cases}
+    groups = {}
+    for c in cases:
+        groups.setdefault(c["P"], []).append(c)
+    solvers, tiles, total_dof, first_dt = [], {}, 0, {}
+    for P in sorted(groups):
+        cs = groups[P]
+        union, grp = concat_meshes([meshes[c["seed"]] for c in cs])
+        s = Solver(union, order=P, dtType=1, precision=FRG_MIXED, **kw)
+        s.set_groups(grp, len(cs))
+        pos = s.get("pos_spts")
+        U = np.empty((s.nSpts, s.nEles, 4))
+        for k, c in enumerate(cs):
+            U[:, grp == k] = vortex_state(pos[:, grp == k], c["eps"], c["mach"])
+        s.set("U_spts", U)
+        s.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            tiles[P] = int(s.autotune(5)[0])
+        solvers.append((P, s, union, grp, U))
+        total_dof += s.nEles * s.nSpts * s.nFields
+    ens = Ensemble([s for _, s, _, _, _ in solvers])
+    ens.set_stream(stream.cuda_stream)
+    ens.update(warmup)
+    for P, s, _, _, _ in solvers:
+        first_dt[P] = s.group_times()[1]
+    ms = timed(lambda: ens.update(nsteps))
+    launches = sum(s.launch_count() for _, s, _, _, _ in solvers)
+    ens.close()
+    ens_rate = total_dof * nsteps / (ms * 1e-3)
+
+    # the same cases one by one (own handle each, graph-replayed steps)
+    alone_ms, alone_dof = 0.0, 0
+    for c in cases:
+        s = Solver(meshes[c["seed"]], order=c["P"], dtType=1, precision=FRG_MIXED, **kw)
+        s.set("U_spts", vortex_state(s.get("pos_spts"), c["eps"], c["mach"]))
+        s.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            s.update(warmup)
+        alone_ms += timed(lambda: s.update(alone_steps))
+        alone_dof += s.nEles * s.nSpts * s.nFields
+        s.set_stream(None)
+        s.close()
+    alone_rate = alone_dof * alone_steps / (alone_ms * 1e-3)
+    for _, s, _, _, _ in solvers:
+        s.set_stream(None)
+        s.close()
+
+    # adjoint of the per-case entropy error, FP64, per order group
+    fwd_ms = adj_ms = 0.0
+    for P, _, union, grp, U in solvers:
+        a = Solver(union, order=P, dtType=0, dt=1.0, precision=FRG_FP64, **kw)
+        a.set_groups(grp, grp.max() + 1, first_dt[P])
+        a.set("U_spts", U)
+        a.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            a.update(1)
+        a.set("U_spts", U)
+        fwd_ms += timed(lambda: a.update(adj_steps))
+        a.set("U_spts", U)
+        with torch.cuda.stream(stream):
+            a.adjoint_forward(adj_steps, 25)
+            a.objective("entropy")
+        adj_ms += timed(lambda: a.adjoint_backward())
+        a.set_stream(None)
+        a.close()
+    return {"workload": "256 isentropic-vortex cases, side {16..96}, P {2..5}, strength U[1,5], Mach U[0.1,0.6], "
+                        "Roe, RK4, per-case CFL 0.5, mixed precision",
+            "cases": len(cases), "cases_per_order": {str(P): len(groups[P]) for P in sorted(groups)},
+            "total_dof": total_dof, "steps": nsteps, "tile_variant_per_order": {str(k): v for k, v in tiles.items()},
+            "ensemble_value": ens_rate, "ensemble_ms_per_step": ms / nsteps, "unit": "DOF-updates/s",
+            "one_by_one_value": alone_rate, "one_by_one_steps_per_case": alone_steps,
+            "ensemble_over_one_by_one": ens_rate / alone_rate,
+            "adjoint_fp64": {"steps": adj_steps, "checkpoint_every": 25, "forward_ms_per_step": fwd_ms / adj_steps,
+                             "adjoint_ms_per_step": adj_ms / adj_steps, "adjoint_over_forward": adj_ms / fwd_ms,
+                             "objective": "per-case entropy error integral at the final time"}}
 
 
 def cpu_baseline(steps=2, threads=1):
@@ -448,6 +577,7 @@ def main():
                 "how": "frg_update_host per step: pinned host state [spt][ele][field] -> device, one RK4 step, "
                        "state -> host"},
         "adjoint": res["adjoint"],
+        "ensemble": res["ensemble"],
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
