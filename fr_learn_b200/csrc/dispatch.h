@@ -29,7 +29,7 @@ struct KernelSet {
     int TE = 0, NT = 0;
     size_t smem = 0;
   };
-  static constexpr int kMaxTma = 4;
+  static constexpr int kMaxTma = 6;
   TmaVariant tma[kMaxTma];
   int nTma = 0;
   int TE = 0;       // elements per block

@@ -1125,6 +1125,12 @@ frg_status frg_set_stream(frg_solver *s, void *stream) {
   return FRG_OK;
 }
 
+frg_status frg_tile_variant_count(const frg_solver *s, int *count) {
+  if (!s || !count) return fail(FRG_ERR_ARG, "null argument");
+  *count = s->useTma ? s->ks.nTma : 1;
+  return FRG_OK;
+}
+
 frg_status frg_set_tile_variant(frg_solver *s, int variant) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
   if (!s->useTma) return variant == 0 ? FRG_OK : fail(FRG_ERR_ARG, "no TMA kernel in use");
@@ -1203,6 +1209,7 @@ frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_
     CK(cudaEventCreate(&e1));
     // three interleaved rounds, the best of each candidate counts, so that a
     // clock ramp or a neighbour's burst does not decide
+    static_assert(KernelSet::kMaxTma <= FRG_MAX_TILE_VARIANTS, "tile variants");
     double msv[KernelSet::kMaxTma];
     for (int v = 0; v < nVar; v++) msv[v] = 1e300;
     for (int round = 0; round < 3 && !st; round++)

@@ -90,7 +90,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Tile of the TMA kernel: TE elements (box inner extent TE * sizeof >= 16 B),
 // NT threads.  TE_ = 0 picks the widest of 16/8/4 elements whose shared
-// memory stays within 72 KB (three blocks per SM); TE_ = -1 half of that.
+// memory stays within 72 KB (three blocks per SM); TE_ = -1 half of that,
+// -2 a quarter (at least 4 elements: the 16-byte TMA box minimum).
 template <class C, typename R, typename S, int TE_ = 0, int NT_ = 128>
 struct TileT {
   static constexpr int NS = C::NS, NF = C::NF, NV = C::NV, D = C::DIM;
@@ -102,10 +103,11 @@ struct TileT {
   }
   static constexpr int PER_ELE = per_ele(0);
   static constexpr int TE_AUTO = (16 * PER_ELE <= 72 * 1024) ? 16 : (8 * PER_ELE <= 72 * 1024) ? 8 : 4;
-  static constexpr int TE = TE_ > 0 ? TE_ : TE_ == 0 ? TE_AUTO : (TE_AUTO > 4 ? TE_AUTO / 2 : 4);
+  static constexpr int TE = TE_ > 0 ? TE_ : TE_ == 0 ? TE_AUTO : TE_ == -1 ? (TE_AUTO > 4 ? TE_AUTO / 2 : 4)
+                                                              : (TE_AUTO > 8 ? TE_AUTO / 4 : 4);
   static constexpr int NT = NT_;
   // blocks per SM the register budget is sized for
-  static constexpr int MINB = NT_ >= 256 ? 2 : NT_ >= 192 ? 2 : 1;
+  static constexpr int MINB = NT_ >= 192 ? 2 : NT_ <= 64 ? 4 : 1;
   static constexpr int al(int b) { return (b + 127) & ~127; }
   // byte offsets of the shared-memory regions (each 128-byte aligned)
   static constexpr int oU0 = 0;
@@ -286,32 +288,49 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
   ok = mbar_wait(&bar[2], 0);
   if (__syncthreads_or(!ok)) goto timeout;
 
-  // ---- phase C: divergence + correction, RK update into the staging tiles
-  for (int it = tid; it < NS * TE; it += NT) {
-    const int s = it / TE, e = it - s * TE, eg = e0 + e;
-    if (eg >= a.nEle) continue;
-    const int i = s % N1, j = (s / N1) % N1, k = DIM == 3 ? s / (N1 * N1) : 0;
-    const int ijk[3] = {i, j, k};
-    int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
-    corr_fpts<C>(i, j, k, cf, cs, ca);
-    const double idet = (double)sDet[s * TE + e];  // 1 / detJ
-    const double dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
+  // ---- phase C: divergence + correction, RK update into the staging tiles.
+  // Along coordinate lines: pass C1 takes the xi-derivative of the xi-flux
+  // along each row j plus the correction from the row's left/right flux
+  // points, for all N1 points of the row at once, into Us (free since phase
+  // B); pass C2 adds the eta part along each column i and does the RK
+  // update of the column's points.  One item = (line, field, element): the
+  // line's N1 values are loaded once and N1 results formed.
+  static_assert(DIM == 2, "the TMA stage kernel is two-dimensional");
+  for (int it = tid; it < N1 * NV * TE; it += NT) {
+    const int e = it % TE, r = it / TE, v = r % NV, j = r / NV;
+    if (e0 + e >= a.nEle) continue;
+    R F[N1];
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
+    for (int q = 0; q < N1; q++) F[q] = Fs[((0 * NV + v) * NS + j * N1 + q) * TE + e];
+    const R JL = Js[(v * NF + 3 * N1 + C::P - j) * TE + e], JR = Js[(v * NF + N1 + j) * TE + e];
+#pragma unroll
+    for (int i = 0; i < N1; i++) {
       R acc = 0;
 #pragma unroll
-      for (int d = 0; d < DIM; d++) {
-        const int sd = d == 0 ? 1 : d == 1 ? N1 : N1 * N1;
-        const int sb = s - ijk[d] * sd;
+      for (int q = 0; q < N1; q++) acc += op.dlag[i][q] * F[q];
+      acc += -op.gL[i] * JL;
+      acc += op.gR[i] * JR;
+      Us[(v * NS + j * N1 + i) * TE + e] = acc;
+    }
+  }
+  __syncthreads();
+  for (int it = tid; it < N1 * NV * TE; it += NT) {
+    const int e = it % TE, r = it / TE, v = r % NV, i = r / NV, eg = e0 + e;
+    if (eg >= a.nEle) continue;
+    const double dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
+    R F[N1];
 #pragma unroll
-        for (int q = 0; q < N1; q++) acc += op.dlag[ijk[d]][q] * Fs[((d * NV + v) * NS + sb + q * sd) * TE + e];
-      }
+    for (int q = 0; q < N1; q++) F[q] = Fs[((1 * NV + v) * NS + q * N1 + i) * TE + e];
+    const R JB = Js[(v * NF + i) * TE + e], JT = Js[(v * NF + 2 * N1 + C::P - i) * TE + e];
 #pragma unroll
-      for (int c = 0; c < 2 * DIM; c++) {
-        const R g = cs[c] ? op.gR[ca[c]] : -op.gL[ca[c]];
-        acc += g * Js[(v * NF + cf[c]) * TE + e];
-      }
-      const int o = (v * NS + s) * TE + e;
+    for (int j = 0; j < N1; j++) {
+      const int s = j * N1 + i, o = (v * NS + s) * TE + e;
+      R acc = Us[o];
+#pragma unroll
+      for (int q = 0; q < N1; q++) acc += op.dlag[j][q] * F[q];
+      acc += -op.gL[j] * JB;
+      acc += op.gR[j] * JT;
+      const double idet = (double)sDet[s * TE + e];  // 1 / detJ
       const double div = (double)acc;
       if (flags & SF_DIVF) a.divF[((size_t)v * NS + s) * a.ldU + eg] = div;
       double unew;
@@ -346,18 +365,24 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
     tma_commit();
   }
 
-  // ---- phase D: traces of the new state, staged in Js
-  for (int it = tid; it < NF * TE; it += NT) {
-    const int f = it / TE, e = it - f * TE;
-    int dir, side, s0, st;
-    fpt_line<C>(f, dir, side, s0, st);
+  // ---- phase D: traces of the new state, staged in Js; one item per
+  // (line, field, element) gives the traces at both ends of the line
+  // (rows: left face 3 / right face 1; columns: bottom face 0 / top face 2)
+  for (int it = tid; it < 2 * N1 * NV * TE; it += NT) {
+    const int e = it % TE, r = it / TE, v = r % NV, ln = r / NV;
+    const bool row = ln < N1;
+    const int k = row ? ln : ln - N1;
+    const int s0 = row ? k * N1 : k, st = row ? 1 : N1;
+    R t0 = 0, t1 = 0;
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
-      R t = 0;
-#pragma unroll
-      for (int j = 0; j < N1; j++) t += op.lag[side][j] * Us[(v * NS + s0 + j * st) * TE + e];
-      reinterpret_cast<S *>(Js)[(v * NF + f) * TE + e] = (S)t;
+    for (int q = 0; q < N1; q++) {
+      const R u = Us[(v * NS + s0 + q * st) * TE + e];
+      t0 += op.lag[0][q] * u;
+      t1 += op.lag[1][q] * u;
     }
+    const int f0 = row ? 3 * N1 + C::P - k : k, f1 = row ? N1 + k : 2 * N1 + C::P - k;
+    reinterpret_cast<S *>(Js)[(v * NF + f0) * TE + e] = (S)t0;
+    reinterpret_cast<S *>(Js)[(v * NF + f1) * TE + e] = (S)t1;
   }
   fence_proxy_async();
   __syncthreads();

@@ -73,8 +73,10 @@ bool make_set(KernelSet &k, std::string &err) {
     k.nTma = 0;
     if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, 0, 128>(k);
     if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, 0, 256>(k);
-    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, 0, 192>(k);
     if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -1, 128>(k);
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -1, 64>(k);
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -2, 64>(k);
+    if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -2, 32>(k);
   }
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;

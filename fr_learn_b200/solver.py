@@ -101,6 +101,7 @@ def lib():
         "frg_time_stages": ([vp, i, vp, C.c_ulonglong, vp], i),
         "frg_autotune": ([vp, i, C.POINTER(C.c_int), vp], i),
         "frg_set_tile_variant": ([vp, i], i),
+        "frg_tile_variant_count": ([vp, C.POINTER(i)], i),
         "frg_objective": ([vp, i, C.POINTER(d), vp], i),
         "frg_set_groups": ([vp, vp, i, vp], i),
         "frg_ensemble_create": ([vp, i, C.POINTER(vp)], i),
@@ -271,9 +272,14 @@ class Solver:
         `nsteps` steps of each candidate; the solution is left unchanged.
         Returns (chosen index, per-candidate ms per step)."""
         v = C.c_int()
-        out = np.zeros(4)
+        out = np.zeros(6)
         _check(lib().frg_autotune(self.h, nsteps, C.byref(v), out.ctypes.data))
-        return v.value, out
+        return v.value, out[:self.tile_variant_count()]
+
+    def tile_variant_count(self):
+        n = C.c_int()
+        _check(lib().frg_tile_variant_count(self.h, C.byref(n)))
+        return n.value
 
     # -- ensemble mode
     def set_groups(self, group_of_element, n_groups, fixed_dt=None):

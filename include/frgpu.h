@@ -202,9 +202,13 @@ frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long
  * of each candidate, then restores the solution, time, dt and iteration the
  * handle had.  Results do not depend on the choice.  `variant_out` receives
  * the chosen index; `ms_out` (may be NULL) one time per step per candidate
- * (up to 4 entries).  A no-op where the TMA kernel is not used.  No
- * counterpart in the reference, which has a single CPU code path. */
+ * (frg_tile_variant_count entries, at most FRG_MAX_TILE_VARIANTS).  A no-op
+ * where the TMA kernel is not used.  No counterpart in the reference, which
+ * has a single CPU code path. */
+#define FRG_MAX_TILE_VARIANTS 6
 frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out);
+/* Number of tile shapes the handle's configuration offers (1 without TMA). */
+frg_status frg_tile_variant_count(const frg_solver *s, int *count);
 /* Selects a tile shape of the TMA stage kernel by index (0 = default). */
 frg_status frg_set_tile_variant(frg_solver *s, int variant);
 /* ---- Ensemble mode (no counterpart in the reference) ---------------------

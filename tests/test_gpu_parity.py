@@ -239,7 +239,9 @@ def test_tile_variants_identical_and_autotune_restores(precision, case):
     else:
         mesh, ic, kw = bump2d(12, 5), 0, dict(order=3, riemannType=1, dtType=1, uBound=0.5 * np.sqrt(1.4), pBound=1.0)
     ref = None
-    for v in range(4):
+    nvar = Solver(mesh, precision=precision, **kw).tile_variant_count()
+    assert nvar == 6
+    for v in range(nvar):
         s = Solver(mesh, precision=precision, **kw)
         s.set_tile_variant(v)
         s.setInitialCondition(ic)
@@ -255,7 +257,7 @@ def test_tile_variants_identical_and_autotune_restores(precision, case):
     s.update(2)
     U2, t2, dt2 = s.get("U_spts"), s.time, s.dt
     v, ms = s.autotune(3)
-    assert 0 <= v < 4 and ms[v] > 0
+    assert 0 <= v < nvar and ms[v] > 0
     assert np.array_equal(s.get("U_spts"), U2) and s.time == t2 and s.dt == dt2
     s.update(2)
     assert np.array_equal(s.get("U_spts"), ref[0])
