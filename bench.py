@@ -238,6 +238,7 @@ def run_gpu(args, rank, world, local_rank):
         sv.set_stream(None)
     res["adjoint"] = run_adjoint_bump(stream)
     res["ensemble"] = run_ensemble(stream)
+    res["tgv"] = run_tgv(stream, flush)
     return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
 
 
@@ -449,6 +450,112 @@ def run_ensemble(stream, nsteps=500, warmup=3, alone_steps=20, adj_steps=100):
                              "objective": "per-case entropy error integral at the final time"}}
 
 
+TGV_N, TGV_P, TGV_MA = 32, 3, 0.1
+TGV_WORKLOAD = "ns3d_taylor_green_periodic_32x32x32_hex_P3_re1600_ma0.1_rusanov_ldg_rk44_dt5e-4"
+
+
+def tgv_mesh():
+    from fr_learn_b200 import box3d
+
+    return box3d(TGV_N, TGV_N, TGV_N, (0.0, 0.0, 0.0), (2 * np.pi,) * 3)
+
+
+def tgv_params(**kw):
+    """Taylor-Green vortex: Re 1600 (rho0 = V0 = L = 1, mu = 1/1600, fixVis),
+    Pr 0.71, Rusanov inviscid flux, LDG viscous flux with penFact 0 and
+    tau 1 (the reference's defaults, src/input.cpp:290-291), RK4, dt 5e-4.
+    At Ma 0.1 the sound speed is 10 V0 and the CFL-1 step of this mesh
+    (ele::calcDt with getCFLLimit(3)) is 9.3e-4: dt 1e-3 diverges within a
+    few dozen steps in the CPU restatement of the reference as well as here,
+    so the workload runs at dt 5e-4 (CFL ~0.54)."""
+    d = dict(order=TGV_P, equation=1, viscous=1, riemannType=0, timeType=4, dtType=0, dt=5e-4, gamma=1.4,
+             mu_inf=1.0 / 1600.0, prandtl=0.71, fixVis=1, penFact=0.0, tau=1.0)
+    d.update(kw)
+    return d
+
+
+def kinetic_energy(U, detJ, P, nDims=3):
+    """Volume-averaged kinetic energy (1/|V|) * integral of rho |u|^2 / 2 by
+    the solution points' Gauss quadrature (tensor-product weights times
+    detJ); U is [spt][ele][field], detJ [spt][ele]."""
+    w1 = np.polynomial.legendre.leggauss(P + 1)[1]
+    w = w1
+    for _ in range(nDims - 1):
+        w = np.multiply.outer(w1, w).reshape(-1)  # spt index i fastest: w[i] * w[j] * w[k]
+    wd = w[:, None] * detJ
+    rho = U[..., 0]
+    ke = 0.5 * (U[..., 1] ** 2 + U[..., 2] ** 2 + U[..., 3] ** 2) / rho
+    return float(np.sum(wd * ke) / np.sum(wd))
+
+
+def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
+    """3D compressible Navier-Stokes Taylor-Green vortex, 32^3 periodic
+    linear hexes, P = 3 (64 solution points per element, 10,485,760 DOF):
+    DOF-updates/s of the mixed and FP64 paths (CUDA events per step, L2
+    flushed before each), per-stage launch times against the byte model, and
+    the kinetic-energy history of both paths over `hist_steps` steps (the
+    dissipation rate -dE_k/dt by central differences of the samples)."""
+    import torch
+
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver
+
+    mesh = tgv_mesh()
+    out = {"workload": TGV_WORKLOAD}
+    hist = {}
+    for name, prec in (("mixed", FRG_MIXED), ("fp64", FRG_FP64)):
+        s = Solver(mesh, precision=prec, **tgv_params())
+        s.set_stream(stream.cuda_stream)
+        s.setInitialCondition(10, TGV_MA)
+        detJ = s.get("detJac_spts")
+        dof = s.nEles * s.nSpts * s.nFields
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                flush.fill_(1)
+                s.update(1)
+            stream.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            l0 = s.launch_count()
+            for k in range(steps):
+                flush.fill_(k & 0xFF)
+                ev[k][0].record(stream)
+                s.update(1)
+                ev[k][1].record(stream)
+            stream.synchronize()
+            ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+            launches = (s.launch_count() - l0) / steps
+            st = s.time_stages(max(3, min(10, steps)), flush.data_ptr(), flush.numel()).tolist()
+        # kinetic-energy history from the initial condition
+        s.setInitialCondition(10, TGV_MA)
+        t_start = s.time
+        ke, tt = [kinetic_energy(s.get("U_spts"), detJ, TGV_P)], [0.0]
+        with torch.cuda.stream(stream):
+            for _ in range(hist_steps // hist_every):
+                s.update(hist_every)
+                stream.synchronize()
+                ke.append(kinetic_energy(s.get("U_spts"), detJ, TGV_P))
+                tt.append(s.time - t_start)
+        hist[name] = (np.array(tt), np.array(ke))
+        b = bytes_per_dof_update(3, TGV_P, 5, 4 if prec == FRG_MIXED else 8, 4 if prec == FRG_MIXED else 8) / 4 * dof
+        st_mean = float(np.mean(st[1:]))
+        out[name] = {"value": dof / (ms * 1e-3), "ms_per_step": ms, "unit": "DOF-updates/s", "dof": dof,
+                     "launches_per_step": launches, "stage_ms": st_mean, "bytes_per_stage": b,
+                     "achieved_gbs": b / (st_mean * 1e-3) / 1e9,
+                     "hbm_frac": b / (st_mean * 1e-3) / 1e9 / peaks()[0]}
+        s.set_stream(None)
+        s.close()
+    (tm, km), (td, kd) = hist["mixed"], hist["fp64"]
+    eps_m = -np.gradient(km, tm)
+    eps_d = -np.gradient(kd, td)
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["kinetic_energy"] = {
+        "t": td.tolist(), "fp64": kd.tolist(), "mixed": km.tolist(),
+        "max_rel_diff": float(np.max(np.abs(km - kd) / kd)),
+        "dissipation_rate_fp64": eps_d.tolist(),
+        "dissipation_rate_max_rel_diff": float(np.max(np.abs(eps_m - eps_d)) / np.max(np.abs(eps_d))),
+    }
+    return out
+
+
 def cpu_baseline(steps=2, threads=1):
     """The oracle (CPU restatement of the reference, which cannot run 2D
     meshes) on the same workload, timed on the host cores."""
@@ -578,6 +685,7 @@ def main():
                        "state -> host"},
         "adjoint": res["adjoint"],
         "ensemble": res["ensemble"],
+        "taylor_green_3d": res["tgv"],
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
