@@ -26,6 +26,10 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
 CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu",
               "adjoint_2d.cu", "adjoint_3d.cu"]
+# The FP32 arithmetic of the mixed mode uses the hardware's approximate
+# single-precision divide and square root (within 2 ulp); FP64 arithmetic is
+# unaffected by these flags, so the FP64 units stay exact.
+UNIT_FLAGS = {u: ["-prec-div=false", "-prec-sqrt=false"] for u in ("stage_2d_f32.cu", "stage_3d_f32.cu")}
 CXX_SOURCES = ["setup.cpp"]
 HEADERS = ["kernels.cuh", "kernels_tma.cuh", "adjoint.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
            "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
@@ -74,7 +78,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or _newer(o, [s] + hdrs):
-            jobs.append([_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o])
+            jobs.append([_nvcc()] + NVCC_FLAGS + UNIT_FLAGS.get(src, []) + (["-Xptxas", "-v"] if verbose else [])
+                        + ["-c", s, "-o", o])
         objs.append(o)
     # the kernel units are independent: compile them in parallel
     from concurrent.futures import ThreadPoolExecutor

@@ -28,8 +28,11 @@ struct KernelSet {
     void (*launch)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
     int TE = 0, NT = 0;
     size_t smem = 0;
+    // persistent variants: launched with (SMs x occ) blocks at most, each
+    // walking tiles with a stride of the grid size
+    int persistent = 0, occ = 0;
   };
-  static constexpr int kMaxTma = 6;
+  static constexpr int kMaxTma = 12;
   TmaVariant tma[kMaxTma];
   int nTma = 0;
   int TE = 0;       // elements per block

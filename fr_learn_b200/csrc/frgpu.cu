@@ -441,7 +441,16 @@ frg_status setup_tma(frg_solver *s) {
       (st = make_map(&s->mDA, s->dAs, ts, es, s->nF, L, TE)) ||
       (st = make_map(&s->mNbr, s->nbr, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, s->nF, L, TE)))
     return st;
-  s->nBlkTma = L / TE;
+  const KernelSet::TmaVariant &tv = s->ks.tma[s->tmaVar];
+  if (tv.persistent) {
+    int dev = 0, nSM = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev));
+    const int nTiles = (s->nE + TE - 1) / TE;
+    s->nBlkTma = std::min(nTiles, nSM * tv.occ);
+  } else {
+    s->nBlkTma = L / TE;
+  }
   return FRG_OK;
 }
 
@@ -543,6 +552,7 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       mm.Win = s->mW[k > 0 ? (k - 1) & 1 : 0];
       mm.Wout = s->mW[k & 1];
       mm.trOut = s->mTr[s->curTr ^ 1];
+      mm.trIn = s->mTr[s->curTr];
       mm.JG = s->mJG;
       mm.det = s->mDet;
       mm.nrm = s->mNrm;
@@ -1543,6 +1553,7 @@ frg_status step_keep_stages(frg_solver *s, double *const *Y, bool advanceTime = 
       mm.Win = first ? s->mW[0] : mY[k];
       mm.Wout = last ? s->mW[0] : mY[k + 1];
       mm.trOut = s->mTr[s->curTr ^ 1];
+      mm.trIn = s->mTr[s->curTr];
       mm.JG = s->mJG;
       mm.det = s->mDet;
       mm.nrm = s->mNrm;

@@ -595,7 +595,7 @@ __device__ __forceinline__ void visc_flux(const R *u, const R *g, R Fv[C::DIM][C
 }
 
 template <class C, typename R, typename S, bool BC>
-__global__ void __launch_bounds__(C::NT, 1) fr_visc_grad_kernel(const StageArgs a) {
+__global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs a) {
   using T = TileV<C, R>;
   constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, NT = C::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -639,7 +639,7 @@ __global__ void __launch_bounds__(C::NT, 1) fr_visc_grad_kernel(const StageArgs 
 }
 
 template <class C, typename R, typename S, bool BC, int RS>
-__global__ void __launch_bounds__(C::NT, 1) fr_stage_visc_kernel(const StageArgs a) {
+__global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs a) {
   using T = TileV<C, R>;
   constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];

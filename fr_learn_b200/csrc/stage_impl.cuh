@@ -34,6 +34,28 @@ cudaError_t add_tma_variant(KernelSet &k) {
     e = cudaFuncSetAttribute(ft, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   return e;
 }
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV, int NB>
+void launch_stage_pipe(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
+  fr_stage_tma_pipe_kernel<C, R, S, BC, RS, TEV, NTV, NB><<<nBlk, NTV, smem, st>>>(
+      *static_cast<const StageArgs *>(args), *static_cast<const TmaMaps *>(maps));
+}
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV, int NB>
+cudaError_t add_pipe_variant(KernelSet &k) {
+  using TT = PipeT<C, R, S, TEV, NTV, NB>;
+  KernelSet::TmaVariant &v = k.tma[k.nTma++];
+  v.launch = &launch_stage_pipe<C, R, S, BC, RS, TEV, NTV, NB>;
+  v.TE = TT::TE;
+  v.NT = NTV;
+  v.smem = TT::SMEM;
+  v.persistent = 1;
+  auto ft = fr_stage_tma_pipe_kernel<C, R, S, BC, RS, TEV, NTV, NB>;
+  cudaError_t e = cudaFuncSetAttribute(ft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ft, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ, ft, NTV, TT::SMEM);
+  if (e == cudaSuccess && v.occ < 1) e = cudaErrorInvalidConfiguration;
+  return e;
+}
 template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage_visc(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_stage_visc_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
@@ -77,6 +99,11 @@ bool make_set(KernelSet &k, std::string &err) {
     if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -1, 64>(k);
     if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -2, 64>(k);
     if (e == cudaSuccess) e = add_tma_variant<C, R, S, BC, RS, -2, 32>(k);
+    // persistent, ring-buffered variants
+    if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 160, 2>(k);
+    if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 160, 3>(k);
+    if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 256, 2>(k);
+    if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 128, 2>(k);
   }
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;
