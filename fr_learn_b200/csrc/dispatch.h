@@ -3,9 +3,11 @@
 // The instantiations live in four translation units (stage_{2d,3d}_{f64,f32}.cu)
 // compiled in parallel; each also owns a copy of the 1D operator tables.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "physics.cuh"
 #include "setup.h"
@@ -67,6 +69,15 @@ bool select_2d_f64(const KernelKey &key, KernelSet &k, std::string &err);
 bool select_2d_f32(const KernelKey &key, KernelSet &k, std::string &err);
 bool select_3d_f64(const KernelKey &key, KernelSet &k, std::string &err);
 bool select_3d_f32(const KernelKey &key, KernelSet &k, std::string &err);
+
+// Tensor-core operator GEMM (opgemm.cu): the operator image (hi/lo TF32
+// halves as K-major core matrices), its shared-memory need, and the launch
+// over a [field][K][ld] float array described by a 3D tensor map with a
+// 128 x KP x 1 box.
+void build_op_image(const double *op, int M, int K, int KP, int NP, std::vector<float> &img);
+size_t op_gemm_smem(int KP, int NP);
+cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
+                           int nEle, int nV, float beta, unsigned *err, cudaStream_t st);
 
 // Uploads the 1D operator tables (all schemes, orders 0..5) into each unit.
 cudaError_t upload_tables_2d_f64();

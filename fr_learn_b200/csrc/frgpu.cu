@@ -247,6 +247,8 @@ struct frg_solver {
   int nBlkTma = 0;
   CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
   AdjState *adj = nullptr;
+  // frg_apply_operator: operator images for the tensor-core GEMM, [which][dim]
+  float *opImg[5][3] = {};
 };
 
 namespace {
@@ -751,6 +753,8 @@ frg_status frg_destroy(frg_solver *s) {
                 s->ticket,
                 s->fvn, s->fvn2};
   for (void *q : vp) if (q) cudaFree(q);
+  for (auto &r : s->opImg)
+    for (float *q : r) if (q) cudaFree(q);
   cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy
   if (own) cudaStreamDestroy(own);
   delete s;
@@ -772,6 +776,43 @@ frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out
   dense_operator(s->p.nDims, s->ops, which, dim, m);
   std::memcpy(out, m.data(), m.size() * sizeof(double));
   return FRG_OK;
+}
+
+frg_status frg_apply_operator(frg_solver *s, int which, int dim, const float *X, float *Y, int ld, float beta) {
+  if (!s || !X || !Y) return fail(FRG_ERR_ARG, "null argument");
+  if (which < 0 || which > 4) return fail(FRG_ERR_ARG, "operator %d does not exist", which);
+  const bool perDim = which == 1 || which == 2 || which == 4;
+  if (dim < 0 || dim >= (perDim ? s->p.nDims : 1)) return fail(FRG_ERR_ARG, "bad operator dimension %d", dim);
+  if (ld < s->nE || ld % 4 || ((uintptr_t)X & 15) || ((uintptr_t)Y & 15))
+    return fail(FRG_ERR_ARG, "arrays must be 16-byte aligned with an element stride >= nEles and a multiple of 4");
+  const int M = (which == 0 || which == 2) ? s->nF : s->nS;
+  const int K = (which == 3 || which == 4) ? s->nF : s->nS;
+  const int KP = (K + 7) & ~7, NP = (M + 15) & ~15;
+  if (NP > 256 || KP > 256 || op_gemm_smem(KP, NP) > 227 * 1024)
+    return fail(FRG_ERR_ARG, "operator %d x %d too large for the single-pass tensor-core kernel", M, K);
+  float *&img = s->opImg[which][dim];
+  if (!img) {
+    std::vector<double> op;
+    dense_operator(s->p.nDims, s->ops, which, dim, op);
+    std::vector<float> h;
+    build_op_image(op.data(), M, K, KP, NP, h);
+    CK(cudaMalloc((void **)&img, h.size() * sizeof(float)));
+    CK(cudaMemcpy(img, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  CUtensorMap mX;
+  cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)K, (cuuint64_t)s->nV};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)ld * 4 * K};
+  cuuint32_t box[3] = {128, (cuuint32_t)KP, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(X), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  CK(launch_op_gemm(mX, img, Y, KP, NP, M, ld, s->nE, s->nV, beta, s->err, s->stream));
+  s->launches++;
+  return check_flags(s);
 }
 
 static frg_status ref_scratch(frg_solver *s, size_t n) {

@@ -1,0 +1,288 @@
+// opgemm.cu -- the FR operator matrices applied as batched dense GEMMs on the
+// 5th-generation tensor cores (tcgen05), fed by TMA, in 3xTF32 split precision
+// with FP32 accumulation in tensor memory.
+//
+// The reference applies every operator of its `oper` object as one row-major
+// dgemm over all elements (oper::applySptsFpts, applyGradSpts,
+// applyExtrapolateFn, applyCorrectDivF, applyCorrectGradU,
+// src/operators.cpp:1191-1450): Y[M][nEles*nFields] = Op[M][K] X[K][...].
+// Here the arrays are [field][point][element] with the element index fastest,
+// so per field Y_v = Op X_v, computed transposed: for a tile of 128 elements,
+//
+//   D[e][m] = sum_k A[e][k] B[k][m],   A = X_v^T (M = elements),
+//   B = Op^T (N = output points)
+//
+// with both operands K-major (8-row x 16-byte core matrices, no swizzle), so
+// the accumulator's TMEM lane is the element and its column the output
+// point: warp w reads lanes 32w..32w+31 and its 32 threads store 32
+// consecutive elements of each output point -- coalesced rows of Y.
+//
+// Split precision: x = hi + lo with hi = tf32(x) (round to nearest) and
+// lo = tf32(x - hi); Op's halves are prepared on the host, X's by the block
+// after the tile lands, which also reorders the tile (points fastest) into
+// the K-major core matrices.  D = A_hi B_hi + A_lo B_hi + A_hi B_lo; the
+// dropped A_lo B_lo term and the rounding of the lo halves are ~2^-21
+// relative.
+//
+// One block per (128-element tile, field): one thread issues the TMA loads
+// (the tile as one [KP][128] box, the operator image as two bulk copies) on
+// one mbarrier, the block splits and reorders the tile, one thread issues the
+// MMAs and commits them to a second mbarrier, and all four warps drain TMEM.
+// Every wait is bounded; on expiry the block flags an error, lets its copies
+// and MMAs land (bounded again), frees its TMEM and returns.  No multicast.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <vector>
+
+#include "dispatch.h"
+#include "kernels_tma.cuh"
+
+namespace frg {
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// Shared-memory matrix descriptor (tcgen05 matrix descriptor): start,
+// leading and stride byte offsets in 16-byte units, version 1 in bits 46-48,
+// layout type 0 (no swizzle) in bits 61-63.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::tf32: F32 accumulator (bits 4-5), TF32 A
+// and B (bits 7-9, 10-12), both K-major (bits 15, 16 clear), N >> 3 in bits
+// 17-22, M >> 4 in bits 24-28 with M = 128.
+__host__ __device__ constexpr uint32_t idesc_tf32(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(accum)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_free(uint32_t tmem, int ncol) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncol) : "memory");
+}
+
+__device__ __forceinline__ void tma_load3d(void *dst, const CUtensorMap *m, int x, int y, int z, uint64_t *b) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(m), "r"(x), "r"(y), "r"(z), "r"(smem_u32(b))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(b))
+               : "memory");
+}
+
+// Y_v = Op X_v (+ beta Y_v) for elements [128 blockIdx.x, +128), field
+// blockIdx.y.  KP: K padded to a multiple of 8; NP: output points padded to a
+// multiple of 16; M: real output points; ncol: TMEM columns allocated (a
+// power of two >= NP).  Bimg: the operator image (see build_op_image).
+// Shared memory: the landed tile [KP][128], A_hi and A_lo as K-major core
+// matrices [KP/8][16][2][8][4], the image, two mbarriers, the TMEM address.
+__global__ void __launch_bounds__(128, 1)
+    fr_op_gemm_tc_kernel(const __grid_constant__ CUtensorMap mX, const float *__restrict__ Bimg, float *Y, int KP,
+                         int NP, int M, int ncol, int ld, int nEle, float beta, unsigned *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char *const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
+  float *St = reinterpret_cast<float *>(sb);
+  float *Ahi = reinterpret_cast<float *>(sb + aBytes);
+  float *Alo = reinterpret_cast<float *>(sb + 2 * aBytes);
+  float *Bs = reinterpret_cast<float *>(sb + 3 * aBytes);  // hi, then lo
+  const uint32_t bHalf = (uint32_t)KP * NP * 4u;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 3 * aBytes + 2 * bHalf);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int e0 = blockIdx.x * 128, v = blockIdx.y;
+
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(ncol)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  if (tid == 0) {
+    mbar_expect_tx(&bar[0], aBytes + 2u * bHalf);
+    tma_load3d(St, &mX, e0, 0, v, &bar[0]);
+    bulk_load(Bs, Bimg, bHalf, &bar[0]);
+    bulk_load(reinterpret_cast<unsigned char *>(Bs) + bHalf, reinterpret_cast<const unsigned char *>(Bimg) + bHalf,
+              bHalf, &bar[0]);
+  }
+  bool ok = mbar_wait(&bar[0], 0);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicOr(err, ERRF_TIMEOUT);
+      mbar_wait(&bar[0], 0);  // bounded: let the copies land
+    }
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, ncol);
+    return;
+  }
+
+  // split and reorder: thread = element e; each group of four consecutive
+  // points becomes one 16-byte row of a core matrix (K step s = k/8, half
+  // h = (k%8)/4, row group g = e/8, row r = e%8)
+  {
+    const int e = tid, g = e >> 3, r = e & 7;
+    for (int q = 0; q < KP / 4; q++) {
+      float4 h, l;
+      h.x = tf32_rna(St[(4 * q + 0) * 128 + e]);
+      h.y = tf32_rna(St[(4 * q + 1) * 128 + e]);
+      h.z = tf32_rna(St[(4 * q + 2) * 128 + e]);
+      h.w = tf32_rna(St[(4 * q + 3) * 128 + e]);
+      l.x = tf32_rna(St[(4 * q + 0) * 128 + e] - h.x);
+      l.y = tf32_rna(St[(4 * q + 1) * 128 + e] - h.y);
+      l.z = tf32_rna(St[(4 * q + 2) * 128 + e] - h.z);
+      l.w = tf32_rna(St[(4 * q + 3) * 128 + e] - h.w);
+      const int o = (q >> 1) * 1024 + g * 64 + (q & 1) * 32 + r * 4;
+      *reinterpret_cast<float4 *>(Ahi + o) = h;
+      *reinterpret_cast<float4 *>(Alo + o) = l;
+    }
+  }
+  fence_proxy_async();
+  __syncthreads();
+
+  if (tid == 0) {
+    tc_fence_after();
+    const uint32_t idesc = idesc_tf32(NP);
+    const uint32_t aHi = smem_u32(Ahi), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
+    // core matrices: the two K halves 128 bytes apart (leading offset), 8-row
+    // groups 256 bytes apart (stride offset); one K step of 8 spans 16 groups
+    // of A (4096 bytes) and NP/8 groups of B (NP*32 bytes)
+    for (int s = 0; s < KP / 8; s++) {
+      const uint64_t ah = smem_desc(aHi + s * 4096, 128, 256);
+      const uint64_t al = smem_desc(aLo + s * 4096, 128, 256);
+      const uint64_t bh = smem_desc(bHi + s * NP * 32, 128, 256);
+      const uint64_t bl = smem_desc(bLo + s * NP * 32, 128, 256);
+      tc_mma(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
+      tc_mma(tmem, al, bh, idesc, 1u);
+      tc_mma(tmem, ah, bl, idesc, 1u);
+    }
+    tc_commit(&bar[1]);
+  }
+  ok = mbar_wait(&bar[1], 0);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicOr(err, ERRF_TIMEOUT);
+      mbar_wait(&bar[1], 0);  // bounded: let the MMAs finish before TMEM is freed
+    }
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, ncol);
+    return;
+  }
+  tc_fence_after();
+
+  // epilogue: lane = element, columns = output points
+  const int e = e0 + 32 * warp + lane;
+  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+  for (int c0 = 0; c0 < NP; c0 += 16) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(trow + (uint32_t)c0));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (e < nEle) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int m = c0 + j;
+        if (m < M) {
+          float *y = Y + ((size_t)v * M + m) * ld + e;
+          const float d = __uint_as_float(r[j]);
+          *y = beta != 0.f ? fmaf(beta, *y, d) : d;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, ncol);
+}
+
+// ---------------------------------------------------------------- host side
+
+static float tf32_round_host(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7F800000u) != 0x7F800000u) u = (u + 0x1000u) & 0xFFFFE000u;  // nearest, ties away from zero
+  else u &= 0xFFFFE000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
+// Operator image for B = Op^T (K-major): for K step s, 8-row group g of
+// output points, K half h: an 8 x 4 core matrix, rows = output points
+// 8g..8g+7, columns = inputs 8s+4h..+3; hi halves first, then lo halves.
+void build_op_image(const double *op, int M, int K, int KP, int NP, std::vector<float> &img) {
+  img.assign((size_t)2 * KP * NP, 0.f);
+  const size_t half = (size_t)KP * NP;
+  for (int s = 0; s < KP / 8; s++)
+    for (int g = 0; g < NP / 8; g++)
+      for (int h = 0; h < 2; h++)
+        for (int r = 0; r < 8; r++)
+          for (int c = 0; c < 4; c++) {
+            const int n = 8 * g + r, k = 8 * s + 4 * h + c;
+            const size_t o = (size_t)s * NP * 8 + (size_t)g * 64 + h * 32 + r * 4 + c;
+            if (n >= M || k >= K) continue;
+            const double x = op[(size_t)n * K + k];
+            const float hi = tf32_round_host((float)x);
+            const float lo = tf32_round_host((float)(x - (double)hi));
+            img[o] = hi;
+            img[half + o] = lo;
+          }
+}
+
+size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 3 + (size_t)2 * KP * NP * 4 + 64 + 1024; }
+
+cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
+                           int nEle, int nV, float beta, unsigned *err, cudaStream_t st) {
+  int ncol = 32;
+  while (ncol < NP) ncol <<= 1;
+  size_t smem = op_gemm_smem(KP, NP);
+  // keep (blocks per SM) x (TMEM columns) within the SM's 512 columns, so a
+  // block never waits for another's allocation
+  const size_t minSmem = (size_t)(227 * 1024) / (size_t)(512 / ncol) + 1;
+  if (smem < minSmem) smem = minSmem;
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((nEle + 127) / 128), (unsigned)nV);
+  fr_op_gemm_tc_kernel<<<grid, 128, smem, st>>>(mX, Bimg, Y, KP, NP, M, ncol, ld, nEle, beta, err);
+  return cudaGetLastError();
+}
+
+}  // namespace frg

@@ -87,6 +87,7 @@ def lib():
         "frg_destroy": ([vp], i),
         "frg_info": ([vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)], i),
         "frg_get_operator": ([vp, i, i, vp], i),
+        "frg_apply_operator": ([vp, i, i, vp, vp, i, C.c_float], i),
         "frg_upload": ([vp, i, vp], i), "frg_download": ([vp, i, i, vp], i),
         "frg_set_initial_condition": ([vp, i, d], i),
         "frg_calc_residual": ([vp, i], i), "frg_time_step_a": ([vp, i, d], i), "frg_time_step_b": ([vp, i], i),
@@ -185,6 +186,11 @@ class Solver:
         out = np.empty(shape, np.float64)
         _check(lib().frg_get_operator(self.h, which, dim, out.ctypes.data))
         return out
+
+    def apply_operator(self, which, dim, X_ptr, Y_ptr, ld, beta=0.0):
+        """Y = Op X + beta Y on FP32 device arrays [nFields][points][ld] (the
+        oper::apply* products as tensor-core GEMMs, see include/frgpu.h)."""
+        _check(lib().frg_apply_operator(self.h, which, dim, X_ptr, Y_ptr, ld, beta))
 
     # -- the reference's entry points
     def setInitialCondition(self, icType=None, a0=0.0):

@@ -128,6 +128,20 @@ frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, i
  * 4 opp_correctU[dim] [nS][nF]. */
 frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out);
 
+/* The operator applications of the `oper` object -- applySptsFpts (which 0),
+ * applyGradSpts (1, one dim), applyExtrapolateFn (2, one dim),
+ * applyCorrectDivF (3), applyCorrectGradU's parent-space product (4, one
+ * dim); src/operators.cpp:1191-1450 -- as batched dense GEMMs on the tensor
+ * cores: Y = Op X + beta Y for every field and element.  X and Y are FP32
+ * DEVICE arrays [nFields][K or M points][ld] (element index fastest, ld >=
+ * nEles a multiple of 4, 16-byte aligned), K/M the operator's input/output
+ * point counts as frg_get_operator shapes them; they must be ready on the
+ * handle's stream (frg_set_stream).  The products are 3xTF32 split precision
+ * with FP32 accumulation (about 1e-6 relative); the call returns when the
+ * kernel has finished.  Operators wider than 256 points, or needing more
+ * than 227 KB of shared memory (3D order 4), are rejected with FRG_ERR_ARG. */
+frg_status frg_apply_operator(frg_solver *s, int which, int dim, const float *X, float *Y, int ld, float beta);
+
 frg_status frg_upload(frg_solver *s, int array, const double *host);
 frg_status frg_download(frg_solver *s, int array, int stage, double *host);
 
