@@ -239,6 +239,7 @@ def run_gpu(args, rank, world, local_rank):
     res["adjoint"] = run_adjoint_bump(stream)
     res["ensemble"] = run_ensemble(stream)
     res["tgv"] = run_tgv(stream, flush)
+    res["opgemm"] = run_operator_gemm(stream, flush)
     return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
 
 
@@ -556,6 +557,52 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
     return out
 
 
+def run_operator_gemm(stream, flush, reps=20):
+    """The oper::apply* products as batched tensor-core GEMMs
+    (frg_apply_operator: tcgen05 MMAs in 3xTF32, TMA-fed tiles) over the
+    Taylor-Green mesh's arrays (32^3 hexes, P = 3, 5 fields, FP32): per
+    operator the kernel time (CUDA events around the launch, L2 flushed
+    before each), the HBM bytes it must move (X read, Y written), and the
+    tensor throughput counting the three TF32 MMAs of each product."""
+    import torch
+
+    from fr_learn_b200 import FRG_MIXED, Solver
+
+    s = Solver(tgv_mesh(), precision=FRG_MIXED, **tgv_params())
+    s.set_stream(stream.cuda_stream)
+    nV, nE, nS, nF = s.nFields, s.nEles, s.nSpts, s.nFpts
+    ld = (nE + 31) // 32 * 32
+    hbm = peaks()[0]
+    out = {"workload": f"{nE} hexes x {nV} fields, P={TGV_P}, FP32 arrays [field][point][element]",
+           "precision": "3xTF32 products, FP32 accumulation in TMEM", "ops": {}}
+    for which, name, (M, K) in ((0, "spts_to_fpts", (nF, nS)), (1, "grad_spts_x", (nS, nS)),
+                                (3, "correction", (nS, nF))):
+        X = torch.randn((nV, K, ld), dtype=torch.float32, device=stream.device)
+        Y = torch.empty((nV, M, ld), dtype=torch.float32, device=stream.device)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                s.apply_operator(which, 0, X.data_ptr(), Y.data_ptr(), ld)
+            s.sync()
+            ms = []
+            for r in range(reps):
+                flush.fill_(r & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                s.apply_operator(which, 0, X.data_ptr(), Y.data_ptr(), ld)
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+            s.sync()
+        t = float(np.median(ms)) * 1e-3
+        byt = 4.0 * nV * nE * (K + M)
+        fl = 2.0 * M * K * nV * nE
+        out["ops"][name] = {"M": M, "K": K, "ms": t * 1e3, "gbs": byt / t / 1e9, "hbm_frac": byt / t / 1e9 / hbm,
+                            "useful_tflops": fl / t / 1e12, "tensor_tflops_3xtf32": 3 * fl / t / 1e12}
+    s.set_stream(None)
+    s.close()
+    return out
+
+
 def cpu_baseline(steps=2, threads=1):
     """The oracle (CPU restatement of the reference, which cannot run 2D
     meshes) on the same workload, timed on the host cores."""
@@ -686,6 +733,7 @@ def main():
         "adjoint": res["adjoint"],
         "ensemble": res["ensemble"],
         "taylor_green_3d": res["tgv"],
+        "operator_gemm_tensor_cores": res["opgemm"],
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }

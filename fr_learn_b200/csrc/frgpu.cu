@@ -812,7 +812,7 @@ frg_status frg_apply_operator(frg_solver *s, int which, int dim, const float *X,
   if (r != CUDA_SUCCESS) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   CK(launch_op_gemm(mX, img, Y, KP, NP, M, ld, s->nE, s->nV, beta, s->err, s->stream));
   s->launches++;
-  return check_flags(s);
+  return FRG_OK;
 }
 
 static frg_status ref_scratch(frg_solver *s, size_t n) {
@@ -1165,7 +1165,7 @@ frg_status frg_set_iter(frg_solver *s, int iter, int initIter) {
 frg_status frg_sync(frg_solver *s) {
   if (!s) return fail(FRG_ERR_ARG, "null handle");
   CK(cudaStreamSynchronize(s->stream));
-  return FRG_OK;
+  return check_flags(s);
 }
 
 frg_status frg_set_stream(frg_solver *s, void *stream) {

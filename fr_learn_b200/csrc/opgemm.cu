@@ -24,16 +24,18 @@
 // dropped A_lo B_lo term and the rounding of the lo halves are ~2^-21
 // relative.
 //
-// One block per (128-element tile, field): one thread issues the TMA loads
-// (the tile as one [KP][128] box, the operator image as two bulk copies) on
-// one mbarrier, the block splits and reorders the tile, one thread issues the
-// MMAs and commits them to a second mbarrier, and all four warps drain TMEM.
+// Persistent blocks over (128-element tile, field) pairs: one thread issues
+// the TMA loads (each tile as one [KP][128] box, the operator image once as
+// two bulk copies) on one mbarrier, the block splits and reorders the tile,
+// one thread issues the next tile's load and this tile's MMAs (committed to a
+// second mbarrier), and all four warps drain TMEM.
 // Every wait is bounded; on expiry the block flags an error, lets its copies
 // and MMAs land (bounded again), frees its TMEM and returns.  No multicast.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -94,15 +96,19 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                : "memory");
 }
 
-// Y_v = Op X_v (+ beta Y_v) for elements [128 blockIdx.x, +128), field
-// blockIdx.y.  KP: K padded to a multiple of 8; NP: output points padded to a
+// Y_v = Op X_v (+ beta Y_v) over tiles of 128 elements of one field; tile t
+// covers elements [128 (t % nT), +128) of field t / nT, nT = ceil(nEle/128).
+// Persistent: block b takes tiles b, b + gridDim.x, ...; the operator image
+// is loaded once, and the next tile's TMA load is issued as soon as the
+// current tile has been split, so it lands while the MMAs and the epilogue
+// run.  KP: K padded to a multiple of 8; NP: output points padded to a
 // multiple of 16; M: real output points; ncol: TMEM columns allocated (a
 // power of two >= NP).  Bimg: the operator image (see build_op_image).
 // Shared memory: the landed tile [KP][128], A_hi and A_lo as K-major core
 // matrices [KP/8][16][2][8][4], the image, two mbarriers, the TMEM address.
 __global__ void __launch_bounds__(128, 1)
     fr_op_gemm_tc_kernel(const __grid_constant__ CUtensorMap mX, const float *__restrict__ Bimg, float *Y, int KP,
-                         int NP, int M, int ncol, int ld, int nEle, float beta, unsigned *err) {
+                         int NP, int M, int ncol, int ld, int nEle, int nV, float beta, unsigned *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char *const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
@@ -114,7 +120,8 @@ __global__ void __launch_bounds__(128, 1)
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 3 * aBytes + 2 * bHalf);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int e0 = blockIdx.x * 128, v = blockIdx.y;
+  const int nT = (nEle + 127) / 128, nTiles = nT * nV;
+  if ((int)blockIdx.x >= nTiles) return;
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -133,99 +140,111 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t tmem = *tslot;
 
   if (tid == 0) {
+    const int t = blockIdx.x;
     mbar_expect_tx(&bar[0], aBytes + 2u * bHalf);
-    tma_load3d(St, &mX, e0, 0, v, &bar[0]);
+    tma_load3d(St, &mX, (t % nT) * 128, 0, t / nT, &bar[0]);
     bulk_load(Bs, Bimg, bHalf, &bar[0]);
     bulk_load(reinterpret_cast<unsigned char *>(Bs) + bHalf, reinterpret_cast<const unsigned char *>(Bimg) + bHalf,
               bHalf, &bar[0]);
   }
-  bool ok = mbar_wait(&bar[0], 0);
-  if (__syncthreads_or(!ok)) {
-    if (tid == 0) {
-      atomicOr(err, ERRF_TIMEOUT);
-      mbar_wait(&bar[0], 0);  // bounded: let the copies land
+  const uint32_t idesc = idesc_tf32(NP);
+  bool ok = true;
+  int j = 0;
+  int loads = 1, loadsDone = 0, mmas = 0, mmasDone = 0;  // thread 0's counts of issued / completed phases
+  for (int t = blockIdx.x; t < nTiles; t += gridDim.x, j++) {
+    const uint32_t par = (uint32_t)(j & 1);
+    ok = mbar_wait(&bar[0], par);
+    if (__syncthreads_or(!ok)) break;
+    loadsDone++;
+    // split and reorder: thread = element e; each group of four consecutive
+    // points becomes one 16-byte row of a core matrix (K step s = k/8, half
+    // h = (k%8)/4, row group g = e/8, row r = e%8).  The previous tile's MMAs
+    // have completed (waited below), so A_hi / A_lo are free.
+    {
+      const int e = tid, g = e >> 3, r = e & 7;
+      for (int q = 0; q < KP / 4; q++) {
+        const float x0 = St[(4 * q + 0) * 128 + e], x1 = St[(4 * q + 1) * 128 + e];
+        const float x2 = St[(4 * q + 2) * 128 + e], x3 = St[(4 * q + 3) * 128 + e];
+        float4 h, l;
+        h.x = tf32_rna(x0);
+        h.y = tf32_rna(x1);
+        h.z = tf32_rna(x2);
+        h.w = tf32_rna(x3);
+        l.x = tf32_rna(x0 - h.x);
+        l.y = tf32_rna(x1 - h.y);
+        l.z = tf32_rna(x2 - h.z);
+        l.w = tf32_rna(x3 - h.w);
+        const int o = (q >> 1) * 1024 + g * 64 + (q & 1) * 32 + r * 4;
+        *reinterpret_cast<float4 *>(Ahi + o) = h;
+        *reinterpret_cast<float4 *>(Alo + o) = l;
+      }
     }
+    fence_proxy_async();
     __syncthreads();
-    if (warp == 0) tmem_free(tmem, ncol);
-    return;
-  }
-
-  // split and reorder: thread = element e; each group of four consecutive
-  // points becomes one 16-byte row of a core matrix (K step s = k/8, half
-  // h = (k%8)/4, row group g = e/8, row r = e%8)
-  {
-    const int e = tid, g = e >> 3, r = e & 7;
-    for (int q = 0; q < KP / 4; q++) {
-      float4 h, l;
-      h.x = tf32_rna(St[(4 * q + 0) * 128 + e]);
-      h.y = tf32_rna(St[(4 * q + 1) * 128 + e]);
-      h.z = tf32_rna(St[(4 * q + 2) * 128 + e]);
-      h.w = tf32_rna(St[(4 * q + 3) * 128 + e]);
-      l.x = tf32_rna(St[(4 * q + 0) * 128 + e] - h.x);
-      l.y = tf32_rna(St[(4 * q + 1) * 128 + e] - h.y);
-      l.z = tf32_rna(St[(4 * q + 2) * 128 + e] - h.z);
-      l.w = tf32_rna(St[(4 * q + 3) * 128 + e] - h.w);
-      const int o = (q >> 1) * 1024 + g * 64 + (q & 1) * 32 + r * 4;
-      *reinterpret_cast<float4 *>(Ahi + o) = h;
-      *reinterpret_cast<float4 *>(Alo + o) = l;
+    if (tid == 0) {
+      // the next tile's load into the now free landing buffer
+      const int tn = t + gridDim.x;
+      if (tn < nTiles) {
+        mbar_expect_tx(&bar[0], aBytes);
+        tma_load3d(St, &mX, (tn % nT) * 128, 0, tn / nT, &bar[0]);
+        loads++;
+      }
+      tc_fence_after();
+      const uint32_t aHi = smem_u32(Ahi), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
+      // core matrices: the two K halves 128 bytes apart (leading offset),
+      // 8-row groups 256 bytes apart (stride offset); one K step of 8 spans
+      // 16 groups of A (4096 bytes) and NP/8 groups of B (NP*32 bytes)
+      for (int s = 0; s < KP / 8; s++) {
+        const uint64_t ah = smem_desc(aHi + s * 4096, 128, 256);
+        const uint64_t al = smem_desc(aLo + s * 4096, 128, 256);
+        const uint64_t bh = smem_desc(bHi + s * NP * 32, 128, 256);
+        const uint64_t bl = smem_desc(bLo + s * NP * 32, 128, 256);
+        tc_mma(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
+        tc_mma(tmem, al, bh, idesc, 1u);
+        tc_mma(tmem, ah, bl, idesc, 1u);
+      }
+      tc_commit(&bar[1]);
+      mmas++;
     }
-  }
-  fence_proxy_async();
-  __syncthreads();
-
-  if (tid == 0) {
+    ok = mbar_wait(&bar[1], par);
+    if (__syncthreads_or(!ok)) break;
+    mmasDone++;
     tc_fence_after();
-    const uint32_t idesc = idesc_tf32(NP);
-    const uint32_t aHi = smem_u32(Ahi), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
-    // core matrices: the two K halves 128 bytes apart (leading offset), 8-row
-    // groups 256 bytes apart (stride offset); one K step of 8 spans 16 groups
-    // of A (4096 bytes) and NP/8 groups of B (NP*32 bytes)
-    for (int s = 0; s < KP / 8; s++) {
-      const uint64_t ah = smem_desc(aHi + s * 4096, 128, 256);
-      const uint64_t al = smem_desc(aLo + s * 4096, 128, 256);
-      const uint64_t bh = smem_desc(bHi + s * NP * 32, 128, 256);
-      const uint64_t bl = smem_desc(bLo + s * NP * 32, 128, 256);
-      tc_mma(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
-      tc_mma(tmem, al, bh, idesc, 1u);
-      tc_mma(tmem, ah, bl, idesc, 1u);
-    }
-    tc_commit(&bar[1]);
-  }
-  ok = mbar_wait(&bar[1], 0);
-  if (__syncthreads_or(!ok)) {
-    if (tid == 0) {
-      atomicOr(err, ERRF_TIMEOUT);
-      mbar_wait(&bar[1], 0);  // bounded: let the MMAs finish before TMEM is freed
-    }
-    __syncthreads();
-    if (warp == 0) tmem_free(tmem, ncol);
-    return;
-  }
-  tc_fence_after();
 
-  // epilogue: lane = element, columns = output points
-  const int e = e0 + 32 * warp + lane;
-  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
-  for (int c0 = 0; c0 < NP; c0 += 16) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(trow + (uint32_t)c0));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (e < nEle) {
+    // epilogue: lane = element, columns = output points
+    const int e = (t % nT) * 128 + 32 * warp + lane, v = t / nT;
+    const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+    for (int c0 = 0; c0 < NP; c0 += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(trow + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (e < nEle) {
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int m = c0 + j;
-        if (m < M) {
-          float *y = Y + ((size_t)v * M + m) * ld + e;
-          const float d = __uint_as_float(r[j]);
-          *y = beta != 0.f ? fmaf(beta, *y, d) : d;
+        for (int q = 0; q < 16; q++) {
+          const int m = c0 + q;
+          if (m < M) {
+            float *y = Y + ((size_t)v * M + m) * ld + e;
+            const float d = __uint_as_float(r[q]);
+            *y = beta != 0.f ? fmaf(beta, *y, d) : d;
+          }
         }
       }
     }
+    // the next tile's MMAs overwrite TMEM only after every warp has read it
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (!ok && tid == 0) {
+    // a bounded wait gave up: flag it and let the load / MMAs in flight
+    // finish (bounded again) before the buffers and TMEM are released
+    atomicOr(err, ERRF_TIMEOUT);
+    for (int q = loadsDone; q < loads; q++) mbar_wait(&bar[0], (uint32_t)(q & 1));
+    for (int q = mmasDone; q < mmas; q++) mbar_wait(&bar[1], (uint32_t)(q & 1));
   }
   tc_fence_before();
   __syncthreads();
@@ -279,9 +298,14 @@ cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, i
   if (smem < minSmem) smem = minSmem;
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, nSM = 0, occ = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fr_op_gemm_tc_kernel, 128, smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((nEle + 127) / 128), (unsigned)nV);
-  fr_op_gemm_tc_kernel<<<grid, 128, smem, st>>>(mX, Bimg, Y, KP, NP, M, ncol, ld, nEle, beta, err);
+  const int nTiles = (nEle + 127) / 128 * nV;
+  const int grid = std::max(1, std::min(nTiles, nSM * std::max(occ, 1)));
+  fr_op_gemm_tc_kernel<<<grid, 128, smem, st>>>(mX, Bimg, Y, KP, NP, M, ncol, ld, nEle, nV, beta, err);
   return cudaGetLastError();
 }
 

@@ -137,9 +137,11 @@ frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out
  * nEles a multiple of 4, 16-byte aligned), K/M the operator's input/output
  * point counts as frg_get_operator shapes them; they must be ready on the
  * handle's stream (frg_set_stream).  The products are 3xTF32 split precision
- * with FP32 accumulation (about 1e-6 relative); the call returns when the
- * kernel has finished.  Operators wider than 256 points, or needing more
- * than 227 KB of shared memory (3D order 4), are rejected with FRG_ERR_ARG. */
+ * with FP32 accumulation (about 1e-6 relative).  The kernel is enqueued on
+ * the handle's stream and the call returns without waiting; frg_sync waits
+ * and reports a kernel's expired bounded wait (FRG_ERR_TIMEOUT).  Operators
+ * wider than 256 points, or needing more than 227 KB of shared memory (3D
+ * order 4), are rejected with FRG_ERR_ARG. */
 frg_status frg_apply_operator(frg_solver *s, int which, int dim, const float *X, float *Y, int ld, float beta);
 
 frg_status frg_upload(frg_solver *s, int array, const double *host);

@@ -56,6 +56,7 @@ def test_apply_operator_matches_dense_fp64(case, which):
         for beta in (0.0, 1.0, -0.5):
             Xd, Yd = X.cuda(), Y0.cuda()
             s.apply_operator(which, dim, Xd.data_ptr(), Yd.data_ptr(), ld, beta)
+            s.sync()
             Y = Yd.cpu().numpy().astype(np.float64)
             Xn, Yn = X.numpy().astype(np.float64), Y0.numpy().astype(np.float64)
             ref = np.einsum("mk,vke->vme", op, Xn[:, :, :nE]) + beta * Yn[:, :, :nE]
@@ -78,6 +79,7 @@ def test_apply_operator_is_more_accurate_than_tf32():
     Xd = X.cuda()
     Yd = torch.zeros((nV, s.nSpts, ld), dtype=torch.float32, device="cuda")
     s.apply_operator(1, 2, Xd.data_ptr(), Yd.data_ptr(), ld)
+    s.sync()
     ref = np.einsum("mk,vke->vme", op, X.numpy().astype(np.float64)[:, :, :nE])
     err = np.abs(Yd.cpu().numpy()[:, :, :nE] - ref).max() / np.abs(ref).max()
     s.set_stream(None)
