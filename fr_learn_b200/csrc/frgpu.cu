@@ -216,6 +216,7 @@ struct frg_solver {
   void *nrm = nullptr, *dAs = nullptr, *JG = nullptr, *detJs = nullptr;
   void *invDetS = nullptr;  // 1 / detJ in the stored type, for the TMA stage kernel
   void *fvn = nullptr, *fvn2 = nullptr;  // viscous: projected viscous flux per flux point
+  void *dUg = nullptr;                   // viscous: corrected gradient at the solution points
   bool visc2 = false;                    // 3D with an LDG penalty: second projection needed
   double *detJd = nullptr, *nrmOwn = nullptr, *dAd = nullptr, *vol = nullptr, *wsurf = nullptr, *wvol = nullptr;
   int *nbr = nullptr;
@@ -542,6 +543,7 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
     a.aNext = jam ? s->RKa[k + 1] : (last ? 0.0 : s->RKa[k + 1]);
     a.bCur = jam ? 0.0 : s->RKb[k];
     a.flags = (last ? SF_WAVESP | SF_LAST | SF_TIME : 0) | (first ? SF_FIRST : 0) | (jam ? SF_JAMESON : 0);
+    a.dUg = s->dUg;
     if (first && s->monitor) {
       a.flags |= SF_DIVF;
       a.divF = s->divF[0];
@@ -644,6 +646,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     s->visc2 = p.nDims == 3 && p.penFact != 0.0;
     if ((st = dalloc_bytes(&s->fvn, nFE * s->sstore))) return st;
     if (s->visc2 && (st = dalloc_bytes(&s->fvn2, nFE * s->sstore))) return st;
+    if ((st = dalloc_bytes(&s->dUg, (size_t)p.nDims * nSE * s->sstore))) return st;
   }
   const int nE = s->nE, L = s->L;
   if ((st = upload_store(s.get(), &s->nrm, pad_rows(s->g.nrmC, nE, L, 0.0))) ||
@@ -751,7 +754,7 @@ frg_status frg_destroy(frg_solver *s) {
   cudaFree(s->grpTime);
   void *vp[] = {s->grp, s->W[0], s->W[1], s->tr[0], s->tr[1], s->nrm, s->dAs, s->JG, s->detJs, s->invDetS, s->nbr, s->err,
                 s->ticket,
-                s->fvn, s->fvn2};
+                s->fvn, s->fvn2, s->dUg};
   for (void *q : vp) if (q) cudaFree(q);
   for (auto &r : s->opImg)
     for (float *q : r) if (q) cudaFree(q);
@@ -992,6 +995,7 @@ frg_status frg_calc_residual(frg_solver *s, int step) {
   a.Uin_d = s->U;
   a.trIn = s->tr[s->curTr];
   a.divF = s->divF[step];
+  a.dUg = s->dUg;
   a.flags = SF_RESIDUAL | SF_WAVESP;
   s->dtFresh = false;  // the wave speeds changed
   if ((st = launch_stage_args(s, a))) return st;

@@ -173,6 +173,10 @@ struct StageArgs {
   void *fvnOut, *fvn2Out;
   const void *fvnIn, *fvn2In;
   int visc2;
+  // viscous path, optional: the corrected physical gradient at the solution
+  // points (S), [DIM][NV][NS][nE], written by the gradient kernel and read by
+  // the stage kernel instead of recomputing it (null: recompute)
+  void *dUg;
   // SF_DTNEXT: the next step's dt (ele::calcDt + the global minimum)
   const double *vol, *dAd, *wsurf;
   double *blockMin, *dtNext, *eleDt;
@@ -613,6 +617,13 @@ __global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs 
   __syncthreads();
   gradient_phase<C, R, S, TE>(a, op, Us, Dc, dUs, e0);
   __syncthreads();
+  if (a.dUg) {  // the gradient for the stage kernel
+    S *dUg = static_cast<S *>(a.dUg);
+    for (int it = threadIdx.x; it < DIM * NV * NS * TE; it += NT) {
+      const int q = it / TE, e = it - q * TE, eg = e0 + e;
+      if (eg < a.nEle) dUg[(size_t)q * a.nE + eg] = (S)dUs[it];
+    }
+  }
   // this side's viscous flux, projected, at every interior flux point
   for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
@@ -657,11 +668,22 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
   const S *fvn2In = static_cast<const S *>(a.fvn2In);
 
   load_state<C, R, S, TE>(a, Us, e0);
-  __syncthreads();
-  ldg_phase<C, R, S, BC, TE>(a, op, Us, Js, e0);
-  __syncthreads();
-  gradient_phase<C, R, S, TE>(a, op, Us, Js, dUs, e0);
-  __syncthreads();
+  if (a.dUg) {
+    // the gradient kernel's corrected gradient (the same values this block
+    // would compute: same inputs, same arithmetic)
+    const S *dUg = static_cast<const S *>(a.dUg);
+    for (int it = tid; it < DIM * NV * NS * TE; it += NT) {
+      const int q = it / TE, e = it - q * TE, eg = e0 + e;
+      if (eg < a.nEle) dUs[it] = (R)dUg[(size_t)q * nE + eg];
+    }
+    __syncthreads();
+  } else {
+    __syncthreads();
+    ldg_phase<C, R, S, BC, TE>(a, op, Us, Js, e0);
+    __syncthreads();
+    gradient_phase<C, R, S, TE>(a, op, Us, Js, dUs, e0);
+    __syncthreads();
+  }
 
   // ---- A: inviscid + viscous flux at solution points, transformed
   // (calcInviscidFlux_spts keeps the physical flux, calcViscousFlux_spts
@@ -731,22 +753,19 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
     R Fn[NV];
     const R ws = inviscid_common<C, R, BC, RS>(UL, UR, n, code, Fn, ph);
     if ((a.flags & SF_WAVESP) && !right && ws >= 0) a.waveSp[(size_t)f * nE + eg] = (double)ws;
-    // this side's viscous flux at the flux point
-    R g[DIM * NV], Fo[DIM][NV];
-    own_grad_trace<C, R, TE>(op, dUs, f, e, g);
-    visc_flux<C, R>(own, g, Fo, ph);
     R nn = 0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) nn += n[d] * n[d];
     const R tau = (R)ph.tau;
     if (code >= 0) {
-      const size_t t = (size_t)(code >> 1);
+      // this side's projected viscous flux: the value the gradient kernel
+      // stored for this flux point (its own trace, gradient trace and
+      // viscousFlux, projected in the same order)
+      const size_t t = (size_t)(code >> 1), me = (size_t)f * nE + eg;
       const R pf = ldg_pen<DIM, R>(n, ph.penFact);
 #pragma unroll
       for (int v = 0; v < NV; v++) {
-        R on = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) on += Fo[d][v] * n[d];
+        const R on = (R)fvnIn[(size_t)v * NF * nE + me];
         const R xn = (R)fvnIn[(size_t)v * NF * nE + t];
         const R FLn = right ? xn : on, FRn = right ? on : xn;
         if constexpr (NV == 1) {
@@ -754,14 +773,20 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
         } else {
           R jumpF = FLn - FRn;
           if constexpr (DIM == 3) {
-            const R al = right ? (a.visc2 ? (R)fvn2In[(size_t)v * NF * nE + t] : xn)
-                               : n[0] * Fo[0][v] + n[1] * Fo[1][v] + n[2] * Fo[1][v];
+            // the left side's n0 F0 + n1 F1 + n2 F1 (src/face.cpp:245); it
+            // only enters multiplied by the penalty factor, so without one
+            // (no second array) any finite value gives the same sum
+            const R al = a.visc2 ? (R)fvn2In[(size_t)v * NF * nE + (right ? t : me)] : (right ? xn : on);
             jumpF = al - FRn;
           }
           Fn[v] += (R)0.5 * (FLn + FRn) + pf * nn * jumpF + tau * nn * (UL[v] - UR[v]);
         }
       }
     } else {
+      // boundary: this side's viscous flux from its gradient trace
+      R g[DIM * NV], Fo[DIM][NV];
+      own_grad_trace<C, R, TE>(op, dUs, f, e, g);
+      visc_flux<C, R>(own, g, Fo, ph);
       if constexpr (NV == 1) {
 #pragma unroll
         for (int d = 0; d < DIM; d++) Fn[0] += (R)0.5 * Fo[d][0] * n[d];  // ghost gradient is zero
