@@ -307,8 +307,11 @@ __device__ __forceinline__ void tma_phase_b(const StageArgs &a, const OpTab<R> &
 // flux points, for all N1 points of the row at once, into Us (free since
 // phase B); pass C2 adds the eta part along each column i and does the RK
 // update of the column's points.  One item = (line, field, element): the
-// line's N1 values are loaded once and N1 results formed.  Contains a block
-// barrier between the passes.
+// line's N1 values are loaded once and N1 results formed.  Items run
+// element-fastest, then line, then field, so the lane groups of a warp
+// fall on different shared-memory banks (the field stride of the flux-point
+// arrays is a multiple of 32 words).  Contains a block barrier between the
+// passes.
 template <class C, typename R, typename S, int TE, int NT>
 __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &op, const TmaBufs<R, S> &b, int e0,
                                             double dtG) {
@@ -317,7 +320,7 @@ __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &
   const int flags = a.flags;
   const bool first = flags & SF_FIRST, last = flags & SF_LAST, jam = flags & SF_JAMESON;
   for (int it = threadIdx.x; it < N1 * NV * TE; it += NT) {
-    const int e = it % TE, r = it / TE, v = r % NV, j = r / NV;
+    const int e = it % TE, r = it / TE, j = r % N1, v = r / N1;
     if (e0 + e >= a.nEle) continue;
     R F[N1];
 #pragma unroll
@@ -335,7 +338,7 @@ __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &
   }
   __syncthreads();
   for (int it = threadIdx.x; it < N1 * NV * TE; it += NT) {
-    const int e = it % TE, r = it / TE, v = r % NV, i = r / NV, eg = e0 + e;
+    const int e = it % TE, r = it / TE, i = r % N1, v = r / N1, eg = e0 + e;
     if (eg >= a.nEle) continue;
     const double dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
     R F[N1];
@@ -382,7 +385,7 @@ template <class C, typename R, typename S, int TE, int NT>
 __device__ __forceinline__ void tma_phase_d(const OpTab<R> &op, const R *Us, S *TrO) {
   constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1;
   for (int it = threadIdx.x; it < 2 * N1 * NV * TE; it += NT) {
-    const int e = it % TE, r = it / TE, v = r % NV, ln = r / NV;
+    const int e = it % TE, r = it / TE, ln = r % (2 * N1), v = r / (2 * N1);
     const bool row = ln < N1;
     const int k = row ? ln : ln - N1;
     const int s0 = row ? k * N1 : k, st = row ? 1 : N1;
