@@ -707,7 +707,7 @@ def main():
     ach = b_mixed / (st_mixed * 1e-3) / 1e9
     ach64 = b_fp64 / (st_fp64 * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "stage_tma_kernel_euler2d_vortex_128x128_P4_traffic.json.txt")
+    tp = os.path.join(ROOT, "profiles", "stage_tma_pipe_kernel_euler2d_vortex_128x128_P4_traffic.json.txt")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
@@ -730,7 +730,8 @@ def main():
         "fp64_density_rel_l2_vs_exact_vortex": errs[2],
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "fr_stage_tma_kernel (mixed)", "launch_ms": st_mixed,
+                     "kernel": ("fr_stage_tma_pipe_kernel" if tiles["mixed"] >= 6 else "fr_stage_tma_kernel")
+                               + f" (mixed, tile variant {tiles['mixed']})", "launch_ms": st_mixed,
                      "bytes_per_launch": b_mixed,
                      "fp64": {"achieved": ach64, "frac": ach64 / peak, "launch_ms": st_fp64,
                               "bytes_per_launch": b_fp64},
