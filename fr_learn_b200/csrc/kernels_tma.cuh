@@ -700,4 +700,230 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
   if (tid == 0) tma_wait_reads();
 }
 
+// ----------------------------------------------------------------------------
+// Split variant: the persistent ring of fr_stage_tma_pipe_kernel with the
+// FP64 step-start state and RK accumulator kept OUT of the ring, in one
+// buffer each per block.  The next tile's U0 (or, in the first stage, its
+// double stage input) is loaded into its buffer as soon as the current
+// tile's phase C has read it; the accumulator, which is a store source, at
+// the start of the next tile once the stores have been read out.  The ring
+// slots shrink by two thirds, so four blocks fit per SM instead of three
+// (and registers are capped to match).  Same per-element arithmetic, hence
+// bit-identical.
+// ----------------------------------------------------------------------------
+template <class C, typename R, typename S, int TEV, int NT_>
+struct SplitT {
+  static constexpr int NS = C::NS, NF = C::NF, NV = C::NV, D = C::DIM;
+  static constexpr int NT = NT_;
+  static constexpr int al(int b) { return (b + 127) & ~127; }
+  static constexpr int slot_bytes(int te) {
+    return al(NV * NS * te * (int)sizeof(R)) + al(D * D * NS * te * (int)sizeof(S)) + al(NS * te * (int)sizeof(S)) +
+           al(D * NF * te * (int)sizeof(S)) + al(NF * te * (int)sizeof(S)) + al(NF * te * 4) +
+           2 * al(NV * NF * te * (int)sizeof(S));
+  }
+  static constexpr int smem_bytes(int te) {
+    return 2 * slot_bytes(te) + 2 * al(NV * NS * te * 8) + al(D * NV * NS * te * (int)sizeof(R)) +
+           al(NV * NF * te * (int)sizeof(R)) + al(NF * te * 8) + al((2 * NF + 1) * te * 8) + 8 * 8 + 128;
+  }
+  // the widest of 16/8/4 elements within 56 KB (four blocks per SM)
+  static constexpr int TE_AUTO = smem_bytes(16) <= 56 * 1024 ? 16 : smem_bytes(8) <= 56 * 1024 ? 8 : 4;
+  static constexpr int TE = TEV > 0 ? TEV : TE_AUTO;
+  static constexpr int oUs = 0;
+  static constexpr int oJG = oUs + al(NV * NS * TE * (int)sizeof(R));
+  static constexpr int oDet = oJG + al(D * D * NS * TE * (int)sizeof(S));
+  static constexpr int oNrm = oDet + al(NS * TE * (int)sizeof(S));
+  static constexpr int oDA = oNrm + al(D * NF * TE * (int)sizeof(S));
+  static constexpr int oNbr = oDA + al(NF * TE * (int)sizeof(S));
+  static constexpr int oTw = oNbr + al(NF * TE * 4);
+  static constexpr int oTr = oTw + al(NV * NF * TE * (int)sizeof(S));
+  static constexpr int SLOT = oTr + al(NV * NF * TE * (int)sizeof(S));
+  static constexpr int oU0 = 2 * SLOT;
+  static constexpr int oAcc = oU0 + al(NV * NS * TE * 8);
+  static constexpr int oFs = oAcc + al(NV * NS * TE * 8);
+  static constexpr int oJs = oFs + al(D * NV * NS * TE * (int)sizeof(R));
+  static constexpr int oWs = oJs + al(NV * NF * TE * (int)sizeof(R));
+  static constexpr int oWd = oWs + al(NF * TE * 8);
+  static constexpr int oBar = oWd + al((2 * NF + 1) * TE * 8);
+  static constexpr int SMEM = oBar + 8 * 8 + 128;
+  static_assert(SMEM == smem_bytes(TE), "layout");
+  static constexpr int MINB = SMEM <= 56 * 1024 && NT <= 160 ? 4 : SMEM <= 75 * 1024 && NT <= 192 ? 3 : 2;
+};
+
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NT>
+__global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
+    fr_stage_tma_split_kernel(const StageArgs a, const __grid_constant__ TmaMaps m) {
+  static_assert(sizeof(R) == sizeof(S), "stage state is loaded straight into the compute buffer");
+  using T = SplitT<C, R, S, TEV, NT>;
+  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, TE = T::TE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char *const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  auto slot = [&](int k) {
+    unsigned char *p = sb + k * T::SLOT;
+    TmaBufs<R, S> b;
+    b.U0 = reinterpret_cast<double *>(sb + T::oU0);
+    b.Acc = reinterpret_cast<double *>(sb + T::oAcc);
+    b.Us = reinterpret_cast<R *>(p + T::oUs);
+    b.JG = reinterpret_cast<S *>(p + T::oJG);
+    b.Det = reinterpret_cast<S *>(p + T::oDet);
+    b.Nrm = reinterpret_cast<S *>(p + T::oNrm);
+    b.DA = reinterpret_cast<S *>(p + T::oDA);
+    b.Nbr = reinterpret_cast<int *>(p + T::oNbr);
+    b.Tw = reinterpret_cast<S *>(p + T::oTw);
+    b.TrO = reinterpret_cast<S *>(p + T::oTr);
+    b.Fs = reinterpret_cast<R *>(sb + T::oFs);
+    b.Js = reinterpret_cast<R *>(sb + T::oJs);
+    b.Ws = reinterpret_cast<double *>(sb + T::oWs);
+    b.Wd = reinterpret_cast<double *>(sb + T::oWd);
+    return b;
+  };
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);  // [2][3] ring groups, then U and Acc
+  uint64_t *barU = bar + 6, *barA = bar + 7;
+
+  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const int tid = threadIdx.x;
+  const int nTiles = (a.nEle + TE - 1) / TE;
+  const int flags = a.flags;
+  const bool last = flags & SF_LAST, jam = flags & SF_JAMESON;
+  const TmaNeeds nd(a);
+  if ((int)blockIdx.x >= nTiles) return;
+
+  // thread 0: a tile's ring groups (0: stage input W, JGinv, codes; 1:
+  // normals, dA, own traces; 2: 1/detJ) into slot k
+  auto issue_slot = [&](const TmaBufs<R, S> &b, int e0, uint64_t *bk) {
+    mbar_expect_tx(&bk[0], (nd.inU ? 0u : (uint32_t)(NV * NS * TE * sizeof(S))) +
+                               (uint32_t)(DIM * DIM * NS * TE * sizeof(S)) + (uint32_t)(NF * TE * 4));
+    if (!nd.inU) tma_load2d(b.Us, &m.Win, e0, 0, &bk[0]);
+    tma_load2d(b.JG, &m.JG, e0, 0, &bk[0]);
+    tma_load2d(b.Nbr, &m.nbr, e0, 0, &bk[0]);
+    mbar_expect_tx(&bk[1], (uint32_t)((DIM * NF * TE + NF * TE + NV * NF * TE) * sizeof(S)));
+    tma_load2d(b.Nrm, &m.nrm, e0, 0, &bk[1]);
+    tma_load2d(b.DA, &m.dA, e0, 0, &bk[1]);
+    tma_load2d(b.Tw, &m.trIn, e0, 0, &bk[1]);
+    mbar_expect_tx(&bk[2], (uint32_t)(NS * TE * sizeof(S)));
+    tma_load2d(b.Det, &m.det, e0, 0, &bk[2]);
+  };
+  // thread 0: the tile's double stage input or U0 (barU), and its RK
+  // accumulator (barA), into the block's FP64 buffers
+  const bool needUg = nd.inU || nd.needU0;
+  auto issue_u = [&](const TmaBufs<R, S> &b, int e0) {
+    mbar_expect_tx(barU, (uint32_t)(NV * NS * TE * 8));
+    tma_load2d(b.U0, &m.U, e0, 0, barU);
+  };
+  auto issue_acc = [&](const TmaBufs<R, S> &b, int e0) {
+    mbar_expect_tx(barA, (uint32_t)(NV * NS * TE * 8));
+    tma_load2d(b.Acc, &m.Acc, e0, 0, barA);
+  };
+
+  if (tid == 0) {
+    for (int i = 0; i < 8; i++) mbar_init(&bar[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    issue_slot(slot(0), blockIdx.x * TE, &bar[0]);
+    if (needUg) issue_u(slot(0), blockIdx.x * TE);
+  }
+  const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
+  double dtMin = INFINITY;
+  bool ok = true;
+  // thread 0's counts of issued and completed phases, for the error path
+  int uIss = needUg ? 1 : 0, uDone = 0, aIss = 0, aDone = 0, sIss = 1;
+  int j = 0;
+  for (;; j++) {
+    const int t = blockIdx.x + j * gridDim.x;
+    if (t >= nTiles) break;
+    const int k = j & 1;
+    const uint32_t par = (uint32_t)((j >> 1) & 1), parF = (uint32_t)(j & 1);
+    const TmaBufs<R, S> b = slot(k);
+    uint64_t *bk = &bar[3 * k];
+    const int e0 = t * TE;
+    if (tid == 0) {
+      // the previous tile's stores have been read out before the FP64
+      // buffers and the other slot are reused
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      if (nd.needAcc) {
+        issue_acc(b, e0);
+        aIss++;
+      }
+      if (needUg && last && j > 0) {  // the buffer was a store source: load only now
+        issue_u(b, e0);
+        uIss++;
+      }
+    }
+    ok = mbar_wait(&bk[0], par);
+    if (nd.inU && ok) {
+      ok = mbar_wait(barU, parF);
+      uDone += ok;
+    }
+    if (__syncthreads_or(!ok)) break;
+    tma_gather<C, S, TE, NT>(a, b.Nbr, b.Js, b.Wd, e0);
+    tma_phase_a<C, R, S, TE, NT>(a, nd.inU, b, e0);
+    if (tid == 0) {
+      const int tn = t + gridDim.x;
+      if (tn < nTiles) {
+        issue_slot(slot(k ^ 1), tn * TE, &bar[3 * (k ^ 1)]);
+        sIss++;
+      }
+    }
+    cp_async_wait_all();
+    ok = mbar_wait(&bk[1], par);
+    if (__syncthreads_or(!ok)) break;
+    tma_phase_b<C, R, S, BC, RS, TE, NT>(a, op, b, e0);
+    ok = mbar_wait(&bk[2], par);
+    if (nd.needU0 && !nd.inU && ok) {
+      ok = mbar_wait(barU, parF);
+      uDone += ok;
+    }
+    if (nd.needAcc && ok) {
+      ok = mbar_wait(barA, parF);
+      aDone += ok;
+    }
+    if (__syncthreads_or(!ok)) break;
+    tma_phase_c<C, R, S, TE, NT>(a, op, b, e0, dtG);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      if (last) tma_store2d(&m.U, e0, 0, b.U0);
+      else {
+        tma_store2d(&m.Wout, e0, 0, b.Us);
+        if (!jam) tma_store2d(&m.Acc, e0, 0, b.Acc);
+      }
+      tma_commit();
+      // the U0 buffer is no longer read (and, outside the last stage, not a
+      // store source): the next tile's double input or U0 can land now
+      const int tn = t + gridDim.x;
+      if (needUg && !last && tn < nTiles) {
+        issue_u(b, tn * TE);
+        uIss++;
+      }
+    }
+    tma_phase_d<C, R, S, TE, NT>(op, b.Us, b.TrO);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store2d(&m.trOut, e0, 0, b.TrO);
+      tma_commit();
+    }
+    if (flags & SF_DTNEXT) dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, b.Wd, e0));
+  }
+  if (!ok) {
+    // a bounded wait gave up: flag it and let every issued load land
+    // (bounded again) before the block's shared memory is released
+    if (tid == 0) {
+      atomicOr(a.err, ERRF_TIMEOUT);
+      for (int q = j; q < sIss; q++)
+        for (int g = 0; g < 3; g++) mbar_wait(&bar[3 * (q & 1) + g], (uint32_t)((q >> 1) & 1));
+      for (int q = uDone; q < uIss; q++) mbar_wait(barU, (uint32_t)(q & 1));
+      for (int q = aDone; q < aIss; q++) mbar_wait(barA, (uint32_t)(q & 1));
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (tid == 0) tma_wait_reads();
+    return;
+  }
+  if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
+  if ((flags & SF_DTNEXT) && tid < 32) tma_dt_reduce(a, dtMin);
+  if (tid == 0) tma_wait_reads();
+}
+
 }  // namespace frg

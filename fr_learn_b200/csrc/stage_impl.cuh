@@ -56,6 +56,28 @@ cudaError_t add_pipe_variant(KernelSet &k) {
   if (e == cudaSuccess && v.occ < 1) e = cudaErrorInvalidConfiguration;
   return e;
 }
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
+void launch_stage_split(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
+  fr_stage_tma_split_kernel<C, R, S, BC, RS, TEV, NTV><<<nBlk, NTV, smem, st>>>(
+      *static_cast<const StageArgs *>(args), *static_cast<const TmaMaps *>(maps));
+}
+template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
+cudaError_t add_split_variant(KernelSet &k) {
+  using TT = SplitT<C, R, S, TEV, NTV>;
+  KernelSet::TmaVariant &v = k.tma[k.nTma++];
+  v.launch = &launch_stage_split<C, R, S, BC, RS, TEV, NTV>;
+  v.TE = TT::TE;
+  v.NT = NTV;
+  v.smem = TT::SMEM;
+  v.persistent = 1;
+  auto ft = fr_stage_tma_split_kernel<C, R, S, BC, RS, TEV, NTV>;
+  cudaError_t e = cudaFuncSetAttribute(ft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ft, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ, ft, NTV, TT::SMEM);
+  if (e == cudaSuccess && v.occ < 1) e = cudaErrorInvalidConfiguration;
+  return e;
+}
 template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage_visc(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_stage_visc_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
@@ -104,6 +126,9 @@ bool make_set(KernelSet &k, std::string &err) {
     if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 160, 3>(k);
     if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 256, 2>(k);
     if (e == cudaSuccess) e = add_pipe_variant<C, R, S, BC, RS, 0, 128, 2>(k);
+    // persistent, FP64 buffers outside the ring (four blocks per SM)
+    if (e == cudaSuccess) e = add_split_variant<C, R, S, BC, RS, 0, 160>(k);
+    if (e == cudaSuccess) e = add_split_variant<C, R, S, BC, RS, 0, 128>(k);
   }
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;

@@ -240,7 +240,7 @@ def test_tile_variants_identical_and_autotune_restores(precision, case):
         mesh, ic, kw = bump2d(12, 5), 0, dict(order=3, riemannType=1, dtType=1, uBound=0.5 * np.sqrt(1.4), pBound=1.0)
     ref = None
     nvar = Solver(mesh, precision=precision, **kw).tile_variant_count()
-    assert nvar == 10
+    assert nvar == 12
     for v in range(nvar):
         s = Solver(mesh, precision=precision, **kw)
         s.set_tile_variant(v)
