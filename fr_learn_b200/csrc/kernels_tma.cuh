@@ -193,7 +193,6 @@ __device__ __forceinline__ void tma_gather(const StageArgs &a, const int *sNbr, 
     if (dtn) {
       cp_async_small<8>(&Wd[it], &a.waveSp[(size_t)f * L + e0 + e]);
       cp_async_small<8>(&Wd[NF * TE + it], &a.dAd[(size_t)f * L + e0 + e]);
-      if (f == 0) cp_async_small<8>(&Wd[2 * NF * TE + e], &a.vol[e0 + e]);
     }
     const int code = sNbr[f * TE + e];
     if (code < 0) continue;
@@ -402,18 +401,18 @@ __device__ __forceinline__ void tma_phase_d(const OpTab<R> &op, const R *Us, S *
   }
 }
 
-// ele::calcDt for element e0 + tid (tid < TE) with the wave speeds this stage
+// ele::calcDt for element e0 + ln (lane ln < TE) with the wave speeds this stage
 // left (src/ele.cpp:1086-1105; flux points summed in order).  Returns the
 // element's dt (INFINITY for other threads); in ensemble mode also reduces
 // into the element's group minimum.
 template <int NF, int TE>
-__device__ __forceinline__ double tma_tile_dt(const StageArgs &a, const double *Ws, const double *Wd, int e0) {
-  const int tid = threadIdx.x, eg = e0 + tid;
-  if (tid >= TE || eg >= a.nEle) return INFINITY;
+__device__ __forceinline__ double tma_tile_dt(const StageArgs &a, const double *Ws, int e0, int ln) {
+  const int eg = e0 + ln;
+  if (ln >= TE || eg >= a.nEle) return INFINITY;
   double iw = 0;
 #pragma unroll
-  for (int f = 0; f < NF; f++) iw += Ws[f * TE + tid];
-  const double dte = a.cflFac * (Wd ? Wd[2 * NF * TE + tid] : a.vol[eg]) / iw;
+  for (int f = 0; f < NF; f++) iw += Ws[f * TE + ln];
+  const double dte = a.cflFac * a.vol[eg] / iw;
   a.eleDt[eg] = dte;
   if (a.grp) {  // ensemble mode: each element into its own group's minimum
     if (!(dte > 1e-13)) atomicOr(a.err, ERRF_DT);
@@ -431,7 +430,7 @@ __device__ __forceinline__ void tma_dt_reduce(const StageArgs &a, double my) {
     const double t = __shfl_xor_sync(0xffffffffu, my, o);
     my = (isnan(t) || t < my) ? t : my;
   }
-  if (threadIdx.x == 0 && !a.grp) {
+  if ((threadIdx.x & 31) == 0 && !a.grp) {
     if (!(my > 1e-13)) atomicOr(a.err, ERRF_DT);  // also catches NaN
     else atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext), (unsigned long long)__double_as_longlong(my));
   }
@@ -515,7 +514,7 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
     tma_store2d(&m.trOut, e0, 0, b.TrO);
     tma_commit();
   }
-  if ((flags & SF_DTNEXT) && tid < 32) tma_dt_reduce(a, tma_tile_dt<NF, TE>(a, b.Ws, b.Wd, e0));
+  if ((flags & SF_DTNEXT) && tid < 32) tma_dt_reduce(a, tma_tile_dt<NF, TE>(a, b.Ws, e0, tid));
   if (tid == 0) tma_wait_reads();
   return;
 
@@ -627,6 +626,8 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
   if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, slot(0), blockIdx.x * TE, &bar[0]);
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   double dtMin = INFINITY;
+  const bool dtn = flags & SF_DTNEXT;
+  int prevE0 = -1;  // the previous tile's first element, for its deferred dt
   int issued = 1;  // tiles whose loads have been issued (thread 0's count)
   bool ok = true;
   int j = 0;
@@ -654,6 +655,10 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
     if (__syncthreads_or(!ok)) break;
     tma_gather<C, S, TE, NT>(a, b.Nbr, b.Js, b.Wd, e0);
     tma_phase_a<C, R, S, TE, NT>(a, nd.inU, b, e0);
+    // the previous tile's ele::calcDt, by the last warp, which phase A's
+    // second round leaves idle; Ws is rewritten only in this tile's phase B
+    if (dtn && prevE0 >= 0 && (tid >> 5) == NT / 32 - 1)
+      dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, prevE0, tid & 31));
     if (NB == 2 && tid == 0) prefetch(j + 1, 0);
     cp_async_wait_all();
     ok = mbar_wait(&bk[1], par);
@@ -679,7 +684,7 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
       tma_store2d(&m.trOut, e0, 0, b.TrO);
       tma_commit();
     }
-    if (flags & SF_DTNEXT) dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, b.Wd, e0));
+    prevE0 = e0;
     // the next tile's phase B rewrites Ws only after the barrier at its start
   }
   if (!ok) {
@@ -696,7 +701,10 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
     return;
   }
   if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
-  if ((flags & SF_DTNEXT) && tid < 32) tma_dt_reduce(a, dtMin);
+  if (dtn && (tid >> 5) == NT / 32 - 1) {
+    if (prevE0 >= 0) dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, slot(0).Ws, prevE0, tid & 31));
+    tma_dt_reduce(a, dtMin);
+  }
   if (tid == 0) tma_wait_reads();
 }
 
@@ -825,6 +833,8 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
   }
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   double dtMin = INFINITY;
+  const bool dtn = flags & SF_DTNEXT;
+  int prevE0 = -1;  // the previous tile's first element, for its deferred dt
   bool ok = true;
   // thread 0's counts of issued and completed phases, for the error path
   int uIss = needUg ? 1 : 0, uDone = 0, aIss = 0, aDone = 0, sIss = 1;
@@ -858,6 +868,10 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     if (__syncthreads_or(!ok)) break;
     tma_gather<C, S, TE, NT>(a, b.Nbr, b.Js, b.Wd, e0);
     tma_phase_a<C, R, S, TE, NT>(a, nd.inU, b, e0);
+    // the previous tile's ele::calcDt, by the last warp, which phase A's
+    // second round leaves idle; Ws is rewritten only in this tile's phase B
+    if (dtn && prevE0 >= 0 && (tid >> 5) == NT / 32 - 1)
+      dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, prevE0, tid & 31));
     if (tid == 0) {
       const int tn = t + gridDim.x;
       if (tn < nTiles) {
@@ -904,7 +918,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
       tma_store2d(&m.trOut, e0, 0, b.TrO);
       tma_commit();
     }
-    if (flags & SF_DTNEXT) dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, b.Wd, e0));
+    prevE0 = e0;
   }
   if (!ok) {
     // a bounded wait gave up: flag it and let every issued load land
@@ -922,7 +936,10 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     return;
   }
   if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
-  if ((flags & SF_DTNEXT) && tid < 32) tma_dt_reduce(a, dtMin);
+  if (dtn && (tid >> 5) == NT / 32 - 1) {
+    if (prevE0 >= 0) dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, slot(0).Ws, prevE0, tid & 31));
+    tma_dt_reduce(a, dtMin);
+  }
   if (tid == 0) tma_wait_reads();
 }
 
