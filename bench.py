@@ -730,7 +730,8 @@ def main():
         "fp64_density_rel_l2_vs_exact_vortex": errs[2],
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": ("fr_stage_tma_pipe_kernel" if tiles["mixed"] >= 6 else "fr_stage_tma_kernel")
+                     "kernel": ("fr_stage_tma_split_kernel" if tiles["mixed"] >= 10 else "fr_stage_tma_pipe_kernel"
+                                if tiles["mixed"] >= 6 else "fr_stage_tma_kernel")
                                + f" (mixed, tile variant {tiles['mixed']})", "launch_ms": st_mixed,
                      "bytes_per_launch": b_mixed,
                      "fp64": {"achieved": ach64, "frac": ach64 / peak, "launch_ms": st_fp64,
