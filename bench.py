@@ -707,7 +707,7 @@ def main():
     ach = b_mixed / (st_mixed * 1e-3) / 1e9
     ach64 = b_fp64 / (st_fp64 * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "stage_tma_pipe_kernel_euler2d_vortex_128x128_P4_traffic.json.txt")
+    tp = os.path.join(ROOT, "profiles", "stage_tma_split_kernel_euler2d_vortex_128x128_P4_traffic.json.txt")
     if os.path.exists(tp):
         try:
             with open(tp) as f:
