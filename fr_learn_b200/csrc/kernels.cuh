@@ -473,6 +473,42 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
 //                         correction, RK update and traces.
 // ----------------------------------------------------------------------------
 
+// L2 prefetch of a block's tile of a [rows][ld] array: one prefetch per
+// row segment (the TE elements of the tile), spread over the block's threads,
+// so the per-thread loads of the phases that follow hit L2.
+template <int TE, int NT>
+__device__ __forceinline__ void prefetch_tile(const void *base, int rows, int ld, int esz, int e0) {
+  const char *p = static_cast<const char *>(base) + (size_t)e0 * esz;
+  for (int r = threadIdx.x; r < rows; r += NT)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p + (size_t)r * ld * esz));
+}
+
+// Prefetch of what a viscous kernel of one RK stage reads for its tile:
+// state, metrics, face data and, for the stage kernel, the gradient, the
+// projected viscous fluxes and the FP64 step-start arrays.
+template <class C, typename S, int TE, int NT>
+__device__ __forceinline__ void prefetch_visc(const StageArgs &a, int e0, bool stage) {
+  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM;
+  const int L = a.nE;
+  if (a.Uin_d) prefetch_tile<TE, NT>(a.Uin_d, NV * NS, a.ldU, 8, e0);
+  else prefetch_tile<TE, NT>(a.Uin_s, NV * NS, a.ldU, (int)sizeof(S), e0);
+  prefetch_tile<TE, NT>(a.JG, DIM * DIM * NS, L, (int)sizeof(S), e0);
+  prefetch_tile<TE, NT>(a.nrm, DIM * NF, L, (int)sizeof(S), e0);
+  prefetch_tile<TE, NT>(a.nbr, NF, L, 4, e0);
+  if (!stage) {
+    prefetch_tile<TE, NT>(a.detJ, NS, L, (int)sizeof(S), e0);
+    return;
+  }
+  prefetch_tile<TE, NT>(a.dA, NF, L, (int)sizeof(S), e0);
+  if (a.dUg) prefetch_tile<TE, NT>(a.dUg, DIM * NV * NS, L, (int)sizeof(S), e0);
+  prefetch_tile<TE, NT>(a.fvnIn, NV * NF, L, (int)sizeof(S), e0);
+  if (!(a.flags & SF_RESIDUAL)) {
+    prefetch_tile<TE, NT>(a.detJ, NS, L, (int)sizeof(S), e0);
+    prefetch_tile<TE, NT>(a.U0, NV * NS, a.ldU, 8, e0);
+    if (!(a.flags & (SF_FIRST | SF_JAMESON))) prefetch_tile<TE, NT>(a.Acc, NV * NS, a.ldU, 8, e0);
+  }
+}
+
 // Elements per block for the viscous kernels (state, jumps, gradient, flux).
 template <class C, typename R>
 struct TileV {
@@ -611,6 +647,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs 
   const S *nrmG = static_cast<const S *>(a.nrm);
   S *fvnOut = static_cast<S *>(a.fvnOut);
   S *fvn2Out = static_cast<S *>(a.fvn2Out);
+  prefetch_visc<C, S, TE, NT>(a, e0, false);
   load_state<C, R, S, TE>(a, Us, e0);
   __syncthreads();
   ldg_phase<C, R, S, BC, TE>(a, op, Us, Dc, e0);
@@ -667,6 +704,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
   const S *fvnIn = static_cast<const S *>(a.fvnIn);
   const S *fvn2In = static_cast<const S *>(a.fvn2In);
 
+  prefetch_visc<C, S, TE, NT>(a, e0, true);
   load_state<C, R, S, TE>(a, Us, e0);
   if (a.dUg) {
     // the gradient kernel's corrected gradient (the same values this block
