@@ -27,8 +27,9 @@
 // Persistent blocks over (128-element tile, field) pairs: one thread issues
 // the TMA loads (each tile as one [KP][128] box, the operator image once as
 // two bulk copies) on one mbarrier, the block splits and reorders the tile,
-// one thread issues the next tile's load and this tile's MMAs (committed to a
-// second mbarrier), and all four warps drain TMEM.
+// one thread issues this tile's MMAs (committed to a second mbarrier) and,
+// once they have read the tile, the next tile's load, and all four warps
+// drain TMEM.
 // Every wait is bounded; on expiry the block flags an error, lets its copies
 // and MMAs land (bounded again), frees its TMEM and returns.  No multicast.
 #include <cuda.h>
@@ -100,24 +101,26 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 // covers elements [128 (t % nT), +128) of field t / nT, nT = ceil(nEle/128).
 // Persistent: block b takes tiles b, b + gridDim.x, ...; the operator image
 // is loaded once, and the next tile's TMA load is issued as soon as the
-// current tile has been split, so it lands while the MMAs and the epilogue
-// run.  KP: K padded to a multiple of 8; NP: output points padded to a
+// current tile's MMAs have read it, so it lands while the accumulator is
+// drained (and while the SM's other block computes).  KP: K padded to a multiple of 8; NP: output points padded to a
 // multiple of 16; M: real output points; ncol: TMEM columns allocated (a
 // power of two >= NP).  Bimg: the operator image (see build_op_image).
-// Shared memory: the landed tile [KP][128], A_hi and A_lo as K-major core
-// matrices [KP/8][16][2][8][4], the image, two mbarriers, the TMEM address.
+// Shared memory: the landed tile [KP][128] (rewritten in place as A_hi),
+// A_lo, both as K-major core matrices [KP/8][16][2][8][4], the image, two
+// mbarriers, the TMEM address: 112 KB for a 64 x 96 operator, two blocks
+// per SM.
 __global__ void __launch_bounds__(128, 1)
     fr_op_gemm_tc_kernel(const __grid_constant__ CUtensorMap mX, const float *__restrict__ Bimg, float *Y, int KP,
                          int NP, int M, int ncol, int ld, int nEle, int nV, float beta, unsigned *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char *const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  unsigned char *const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
-  float *St = reinterpret_cast<float *>(sb);
-  float *Ahi = reinterpret_cast<float *>(sb + aBytes);
-  float *Alo = reinterpret_cast<float *>(sb + 2 * aBytes);
-  float *Bs = reinterpret_cast<float *>(sb + 3 * aBytes);  // hi, then lo
+  float *St = reinterpret_cast<float *>(sb);  // the landed tile, turned into A_hi in place
+  float *Ahi = St;
+  float *Alo = reinterpret_cast<float *>(sb + aBytes);
+  float *Bs = reinterpret_cast<float *>(sb + 2 * aBytes);  // hi, then lo
   const uint32_t bHalf = (uint32_t)KP * NP * 4u;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 3 * aBytes + 2 * bHalf);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 2 * aBytes + 2 * bHalf);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nT = (nEle + 127) / 128, nTiles = nT * nV;
@@ -158,37 +161,38 @@ __global__ void __launch_bounds__(128, 1)
     loadsDone++;
     // split and reorder: thread = element e; each group of four consecutive
     // points becomes one 16-byte row of a core matrix (K step s = k/8, half
-    // h = (k%8)/4, row group g = e/8, row r = e%8).  The previous tile's MMAs
-    // have completed (waited below), so A_hi / A_lo are free.
+    // h = (k%8)/4, row group g = e/8, row r = e%8).  The core matrices of K
+    // step s occupy exactly the bytes of landed rows 8s..8s+7, so A_hi is
+    // written in place, one 8-row block at a time: every thread reads its
+    // column of the block, the block synchronises, then the block is
+    // rewritten.  The previous tile's MMAs have completed (waited below).
     {
       const int e = tid, g = e >> 3, r = e & 7;
-      for (int q = 0; q < KP / 4; q++) {
-        const float x0 = St[(4 * q + 0) * 128 + e], x1 = St[(4 * q + 1) * 128 + e];
-        const float x2 = St[(4 * q + 2) * 128 + e], x3 = St[(4 * q + 3) * 128 + e];
-        float4 h, l;
-        h.x = tf32_rna(x0);
-        h.y = tf32_rna(x1);
-        h.z = tf32_rna(x2);
-        h.w = tf32_rna(x3);
-        l.x = tf32_rna(x0 - h.x);
-        l.y = tf32_rna(x1 - h.y);
-        l.z = tf32_rna(x2 - h.z);
-        l.w = tf32_rna(x3 - h.w);
-        const int o = (q >> 1) * 1024 + g * 64 + (q & 1) * 32 + r * 4;
-        *reinterpret_cast<float4 *>(Ahi + o) = h;
-        *reinterpret_cast<float4 *>(Alo + o) = l;
+      for (int sk = 0; sk < KP / 8; sk++) {
+        float x[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) x[c] = St[(8 * sk + c) * 128 + e];
+        __syncthreads();
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+          float4 h, l;
+          h.x = tf32_rna(x[4 * hh + 0]);
+          h.y = tf32_rna(x[4 * hh + 1]);
+          h.z = tf32_rna(x[4 * hh + 2]);
+          h.w = tf32_rna(x[4 * hh + 3]);
+          l.x = tf32_rna(x[4 * hh + 0] - h.x);
+          l.y = tf32_rna(x[4 * hh + 1] - h.y);
+          l.z = tf32_rna(x[4 * hh + 2] - h.z);
+          l.w = tf32_rna(x[4 * hh + 3] - h.w);
+          const int o = sk * 1024 + g * 64 + hh * 32 + r * 4;
+          *reinterpret_cast<float4 *>(Ahi + o) = h;
+          *reinterpret_cast<float4 *>(Alo + o) = l;
+        }
       }
     }
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      // the next tile's load into the now free landing buffer
-      const int tn = t + gridDim.x;
-      if (tn < nTiles) {
-        mbar_expect_tx(&bar[0], aBytes);
-        tma_load3d(St, &mX, (tn % nT) * 128, 0, tn / nT, &bar[0]);
-        loads++;
-      }
       tc_fence_after();
       const uint32_t aHi = smem_u32(Ahi), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
       // core matrices: the two K halves 128 bytes apart (leading offset),
@@ -209,6 +213,16 @@ __global__ void __launch_bounds__(128, 1)
     ok = mbar_wait(&bar[1], par);
     if (__syncthreads_or(!ok)) break;
     mmasDone++;
+    if (tid == 0) {
+      // the MMAs have read A_hi: the next tile can land in its place while
+      // the accumulator is drained
+      const int tn = t + gridDim.x;
+      if (tn < nTiles) {
+        mbar_expect_tx(&bar[0], aBytes);
+        tma_load3d(St, &mX, (tn % nT) * 128, 0, tn / nT, &bar[0]);
+        loads++;
+      }
+    }
     tc_fence_after();
 
     // epilogue: lane = element, columns = output points
@@ -285,7 +299,7 @@ void build_op_image(const double *op, int M, int K, int KP, int NP, std::vector<
           }
 }
 
-size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 3 + (size_t)2 * KP * NP * 4 + 64 + 1024; }
+size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 2 + (size_t)2 * KP * NP * 4 + 64 + 128; }
 
 cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
                            int nEle, int nV, float beta, unsigned *err, cudaStream_t st) {
@@ -298,6 +312,9 @@ cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, i
   if (smem < minSmem) smem = minSmem;
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
   int dev = 0, nSM = 0, occ = 0;
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev);
