@@ -38,6 +38,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "dispatch.h"
@@ -311,14 +313,31 @@ cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, i
   const size_t minSmem = (size_t)(227 * 1024) / (size_t)(512 / ncol) + 1;
   if (smem < minSmem) smem = minSmem;
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
-  int dev = 0, nSM = 0, occ = 0;
-  if (e == cudaSuccess) e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fr_op_gemm_tc_kernel, 128, smem);
+  // per device, once: the kernel's shared-memory limit and carveout, and the
+  // SM count (host calls kept off the per-launch path)
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<int, int> smCount;
+  int nSM = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = smCount.find(dev);
+    if (it == smCount.end()) {
+      e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fr_op_gemm_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      smCount[dev] = nSM;
+    } else {
+      nSM = it->second;
+    }
+  }
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fr_op_gemm_tc_kernel, 128, smem);
   if (e != cudaSuccess) return e;
   const int nTiles = (nEle + 127) / 128 * nV;
   const int grid = std::max(1, std::min(nTiles, nSM * std::max(occ, 1)));
