@@ -240,14 +240,16 @@ __global__ void __launch_bounds__(128, 1)
           : "r"(trow + (uint32_t)c0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (e < nEle) {
+        float *y = Y + ((size_t)v * M + c0) * ld + e;
+        const int nq = min(16, M - c0);
+        if (beta == 0.f) {  // plain stores: no read of Y
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-          const int m = c0 + q;
-          if (m < M) {
-            float *y = Y + ((size_t)v * M + m) * ld + e;
-            const float d = __uint_as_float(r[q]);
-            *y = beta != 0.f ? fmaf(beta, *y, d) : d;
-          }
+          for (int q = 0; q < 16; q++)
+            if (q < nq) __stcs(y + (size_t)q * ld, __uint_as_float(r[q]));
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; q++)
+            if (q < nq) y[(size_t)q * ld] = fmaf(beta, y[(size_t)q * ld], __uint_as_float(r[q]));
         }
       }
     }
