@@ -67,13 +67,23 @@ struct Cfg {
   static constexpr int NFF = DIM == 2 ? N1 : N1 * N1;
   static constexpr int NF = 2 * DIM * NFF;
   static constexpr int NT = 256;  // threads per block
+  // Shared-memory slot of solution point s in the per-point tile arrays.  In
+  // 3D one empty slot follows every coordinate line along xi, so the points
+  // that start the lines of a face (4 apart at P = 3) fall on different
+  // shared-memory banks instead of one (2D: no padding).
+  static constexpr int NSP = DIM == 3 ? NS + NS / N1 : NS;
 };
+template <class C>
+__device__ __forceinline__ constexpr int sx(int s) {
+  if constexpr (C::DIM == 3) return s + s / C::N1;
+  else return s;
+}
 
 // Elements per block: as many as fit ~100 KB of shared memory (two blocks per
 // SM), capped at 32 so a warp spans 32 elements of one point.
 template <class C, typename R>
 struct Tile {
-  static constexpr int PER_ELE = (C::NV * C::NS + C::DIM * C::NV * C::NS + C::NV * C::NF) * (int)sizeof(R);
+  static constexpr int PER_ELE = (C::NV * C::NSP + C::DIM * C::NV * C::NSP + C::NV * C::NF) * (int)sizeof(R);
   static constexpr int TE = (32 * PER_ELE <= 100 * 1024) ? 32 : (16 * PER_ELE <= 100 * 1024) ? 16
                             : (8 * PER_ELE <= 110 * 1024) ? 8 : 4;
   static constexpr int SMEM = TE * PER_ELE;
@@ -249,7 +259,7 @@ __device__ __forceinline__ R inviscid_common(const R *UL, const R *UR, const R *
 // Phase A0: the tile's stage state into shared memory.
 template <class C, typename R, typename S, int TE>
 __device__ __forceinline__ void load_state(const StageArgs &a, R *Us, int e0) {
-  constexpr int NS = C::NS, NV = C::NV, NT = C::NT;
+  constexpr int NS = C::NS, NSP = C::NSP, NV = C::NV, NT = C::NT;
   const S *Uin_s = static_cast<const S *>(a.Uin_s);
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
     const int s = it / TE, e = it - s * TE, eg = e0 + e;
@@ -257,7 +267,7 @@ __device__ __forceinline__ void load_state(const StageArgs &a, R *Us, int e0) {
 #pragma unroll
     for (int v = 0; v < NV; v++) {
       const size_t gi = ((size_t)v * NS + s) * a.ldU + eg;
-      Us[(v * NS + s) * TE + e] = a.Uin_d ? (R)a.Uin_d[gi] : (R)Uin_s[gi];
+      Us[(v * NSP + sx<C>(s)) * TE + e] = a.Uin_d ? (R)a.Uin_d[gi] : (R)Uin_s[gi];
     }
   }
 }
@@ -267,7 +277,7 @@ __device__ __forceinline__ void load_state(const StageArgs &a, R *Us, int e0) {
 template <class C, typename R, typename S, int TE>
 __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> &op, const R *Fs, const R *Js, R *Us,
                                              int e0) {
-  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  constexpr int NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   const S *detJG = static_cast<const S *>(a.detJ);
   S *Wout = static_cast<S *>(a.Wout);
   const int nE = a.nE;
@@ -293,7 +303,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
         const int sd = d == 0 ? 1 : d == 1 ? N1 : N1 * N1;
         const int sb = s - ijk[d] * sd;
 #pragma unroll
-        for (int q = 0; q < N1; q++) acc += op.dlag[ijk[d]][q] * Fs[((d * NV + v) * NS + sb + q * sd) * TE + e];
+        for (int q = 0; q < N1; q++) acc += op.dlag[ijk[d]][q] * Fs[((d * NV + v) * NSP + sx<C>(sb + q * sd)) * TE + e];
       }
 #pragma unroll
       for (int c = 0; c < 2 * DIM; c++) {
@@ -324,7 +334,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
         }
       }
       if (last && (v == 0 || v == NV - 1) && isnan(unew)) atomicOr(a.err, ERRF_NAN);
-      Us[(v * NS + s) * TE + e] = (R)(last ? unew : (double)(S)unew);
+      Us[(v * NSP + sx<C>(s)) * TE + e] = (R)(last ? unew : (double)(S)unew);
     }
   }
   if (!resid && !a.grp && (a.flags & SF_TIME) && blockIdx.x == 0 && threadIdx.x == 0) *a.time += a.dt[0];
@@ -333,7 +343,7 @@ __device__ __forceinline__ void update_phase(const StageArgs &a, const OpTab<R> 
 // Phase D: traces of the new state for the next launch.
 template <class C, typename R, typename S, int TE>
 __device__ __forceinline__ void trace_phase(const StageArgs &a, const OpTab<R> &op, const R *Us, int e0) {
-  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1, NT = C::NT;
+  constexpr int NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, N1 = C::N1, NT = C::NT;
   S *trOut = static_cast<S *>(a.trOut);
   for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE, eg = e0 + e;
@@ -344,7 +354,7 @@ __device__ __forceinline__ void trace_phase(const StageArgs &a, const OpTab<R> &
     for (int v = 0; v < NV; v++) {
       R t = 0;
 #pragma unroll
-      for (int j = 0; j < N1; j++) t += op.lag[side][j] * Us[(v * NS + s0 + j * st) * TE + e];
+      for (int j = 0; j < N1; j++) t += op.lag[side][j] * Us[(v * NSP + sx<C>(s0 + j * st)) * TE + e];
       trOut[((size_t)v * NF + f) * a.nE + eg] = (S)t;
     }
   }
@@ -359,7 +369,7 @@ __device__ __forceinline__ void own_trace(const OpTab<R> &op, const R *Us, int f
   for (int v = 0; v < C::NV; v++) {
     R t = 0;
 #pragma unroll
-    for (int j = 0; j < C::N1; j++) t += op.lag[side][j] * Us[(v * C::NS + s0 + j * st) * TE + e];
+    for (int j = 0; j < C::N1; j++) t += op.lag[side][j] * Us[(v * C::NSP + sx<C>(s0 + j * st)) * TE + e];
     out[v] = t;
   }
 }
@@ -371,11 +381,11 @@ __device__ __forceinline__ void own_trace(const OpTab<R> &op, const R *Us, int f
 template <class C, typename R, typename S, bool BC, int RS>
 __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
   using T = Tile<C, R>;
-  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  constexpr int TE = T::TE, NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
-  R *Fs = Us + NV * NS * TE;                // [DIM][NV][NS][TE]
-  R *Js = Fs + DIM * NV * NS * TE;          // [NV][NF][TE]
+  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NSP][TE]
+  R *Fs = Us + NV * NSP * TE;               // [DIM][NV][NSP][TE]
+  R *Js = Fs + DIM * NV * NSP * TE;         // [NV][NF][TE]
   const OpTab<R> &op = optab<R>(a.vcjh, C::P);
   const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
   const Phys &ph = a.ph;
@@ -391,7 +401,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
     if (eg >= a.nEle) continue;
     R u[NV];
 #pragma unroll
-    for (int v = 0; v < NV; v++) u[v] = Us[(v * NS + s) * TE + e];
+    for (int v = 0; v < NV; v++) u[v] = Us[(v * NSP + sx<C>(s)) * TE + e];
     R F[DIM][NV];
     inviscid_flux<DIM, NV, R>(u, F, ph);
     R G[DIM][DIM];
@@ -406,7 +416,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
         R t = 0;
 #pragma unroll
         for (int d2 = 0; d2 < DIM; d2++) t += G[d1][d2] * F[d2][v];
-        Fs[((d1 * NV + v) * NS + s) * TE + e] = t;
+        Fs[((d1 * NV + v) * NSP + sx<C>(s)) * TE + e] = t;
       }
   }
   __syncthreads();
@@ -424,8 +434,8 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
 #pragma unroll
       for (int j = 0; j < N1; j++) {
         const R l = op.lag[side][j];
-        t += l * Us[(v * NS + s0 + j * st) * TE + e];
-        q += l * Fs[((dir * NV + v) * NS + s0 + j * st) * TE + e];
+        t += l * Us[(v * NSP + sx<C>(s0 + j * st)) * TE + e];
+        q += l * Fs[((dir * NV + v) * NSP + sx<C>(s0 + j * st)) * TE + e];
       }
       own[v] = t;
       dis[v] = side ? q : -q;
@@ -488,7 +498,7 @@ __device__ __forceinline__ void prefetch_tile(const void *base, int rows, int ld
 // projected viscous fluxes and the FP64 step-start arrays.
 template <class C, typename S, int TE, int NT>
 __device__ __forceinline__ void prefetch_visc(const StageArgs &a, int e0, bool stage) {
-  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM;
+  constexpr int NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, DIM = C::DIM;
   const int L = a.nE;
   if (a.Uin_d) prefetch_tile<TE, NT>(a.Uin_d, NV * NS, a.ldU, 8, e0);
   else prefetch_tile<TE, NT>(a.Uin_s, NV * NS, a.ldU, (int)sizeof(S), e0);
@@ -512,7 +522,7 @@ __device__ __forceinline__ void prefetch_visc(const StageArgs &a, int e0, bool s
 // Elements per block for the viscous kernels (state, jumps, gradient, flux).
 template <class C, typename R>
 struct TileV {
-  static constexpr int PER_ELE = (C::NV * C::NS + C::NV * C::NF + 2 * C::DIM * C::NV * C::NS) * (int)sizeof(R);
+  static constexpr int PER_ELE = (C::NV * C::NSP + C::NV * C::NF + 2 * C::DIM * C::NV * C::NSP) * (int)sizeof(R);
   static constexpr int TE = (32 * PER_ELE <= 100 * 1024) ? 32 : (16 * PER_ELE <= 100 * 1024) ? 16
                             : (8 * PER_ELE <= 110 * 1024) ? 8 : 4;
   static constexpr int SMEM = TE * PER_ELE;
@@ -561,11 +571,11 @@ __device__ __forceinline__ void ldg_phase(const StageArgs &a, const OpTab<R> &op
 
 // C1: physical gradient at solution points: D U + correction by the common
 // solution (calcGradU_spts, correctGradU src/solver.cpp:808-879), then
-// JGinv^T / detJ.  dUs is [DIM][NV][NS][TE].
+// JGinv^T / detJ.  dUs is [DIM][NV][NSP][TE] (point slots sx<C>(s)).
 template <class C, typename R, typename S, int TE>
 __device__ __forceinline__ void gradient_phase(const StageArgs &a, const OpTab<R> &op, const R *Us, const R *Dc,
                                                R *dUs, int e0) {
-  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  constexpr int NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   const S *JGG = static_cast<const S *>(a.JG);
   const S *detJG = static_cast<const S *>(a.detJ);
   for (int it = threadIdx.x; it < NS * TE; it += NT) {
@@ -590,7 +600,7 @@ __device__ __forceinline__ void gradient_phase(const StageArgs &a, const OpTab<R
         const int sb = s - ijk[d] * sd;
         R acc = 0;
 #pragma unroll
-        for (int q = 0; q < N1; q++) acc += op.dlag[ijk[d]][q] * Us[(v * NS + sb + q * sd) * TE + e];
+        for (int q = 0; q < N1; q++) acc += op.dlag[ijk[d]][q] * Us[(v * NSP + sx<C>(sb + q * sd)) * TE + e];
 #pragma unroll
         for (int c = 0; c < 2 * DIM; c++)
           if (face_dir<C>(c) == d) acc += (cs[c] ? op.gR[ca[c]] : op.gL[ca[c]]) * Dc[(v * NF + cf[c]) * TE + e];
@@ -601,7 +611,7 @@ __device__ __forceinline__ void gradient_phase(const StageArgs &a, const OpTab<R
         R t = 0;
 #pragma unroll
         for (int d2 = 0; d2 < DIM; d2++) t += gr[d2] * G[d2][d1];
-        dUs[((d1 * NV + v) * NS + s) * TE + e] = invDet * t;
+        dUs[((d1 * NV + v) * NSP + sx<C>(s)) * TE + e] = invDet * t;
       }
     }
   }
@@ -616,7 +626,7 @@ __device__ __forceinline__ void own_grad_trace(const OpTab<R> &op, const R *dUs,
   for (int q = 0; q < C::DIM * C::NV; q++) {
     R t = 0;
 #pragma unroll
-    for (int j = 0; j < C::N1; j++) t += op.lag[side][j] * dUs[(q * C::NS + s0 + j * st) * TE + e];
+    for (int j = 0; j < C::N1; j++) t += op.lag[side][j] * dUs[(q * C::NSP + sx<C>(s0 + j * st)) * TE + e];
     g[q] = t;
   }
 }
@@ -637,11 +647,11 @@ __device__ __forceinline__ void visc_flux(const R *u, const R *g, R Fv[C::DIM][C
 template <class C, typename R, typename S, bool BC>
 __global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs a) {
   using T = TileV<C, R>;
-  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, NT = C::NT;
+  constexpr int TE = T::TE, NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, DIM = C::DIM, NT = C::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
-  R *Dc = Us + NV * NS * TE;                // [NV][NF][TE]
-  R *dUs = Dc + NV * NF * TE;               // [DIM][NV][NS][TE]
+  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NSP][TE]
+  R *Dc = Us + NV * NSP * TE;               // [NV][NF][TE]
+  R *dUs = Dc + NV * NF * TE;               // [DIM][NV][NSP][TE]
   const OpTab<R> &op = optab<R>(a.vcjh, C::P);
   const int e0 = blockIdx.x * TE;
   const S *nrmG = static_cast<const S *>(a.nrm);
@@ -658,7 +668,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs 
     S *dUg = static_cast<S *>(a.dUg);
     for (int it = threadIdx.x; it < DIM * NV * NS * TE; it += NT) {
       const int q = it / TE, e = it - q * TE, eg = e0 + e;
-      if (eg < a.nEle) dUg[(size_t)q * a.nE + eg] = (S)dUs[it];
+      if (eg < a.nEle) dUg[(size_t)q * a.nE + eg] = (S)dUs[((q / NS) * NSP + sx<C>(q % NS)) * TE + e];
     }
   }
   // this side's viscous flux, projected, at every interior flux point
@@ -689,12 +699,12 @@ __global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs 
 template <class C, typename R, typename S, bool BC, int RS>
 __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs a) {
   using T = TileV<C, R>;
-  constexpr int TE = T::TE, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
+  constexpr int TE = T::TE, NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1, NT = C::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NS][TE]
-  R *Js = Us + NV * NS * TE;                // [NV][NF][TE]: dUc, then the jumps
-  R *dUs = Js + NV * NF * TE;               // [DIM][NV][NS][TE]
-  R *Fs = dUs + DIM * NV * NS * TE;         // [DIM][NV][NS][TE]
+  R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NSP][TE]
+  R *Js = Us + NV * NSP * TE;               // [NV][NF][TE]: dUc, then the jumps
+  R *dUs = Js + NV * NF * TE;               // [DIM][NV][NSP][TE]
+  R *Fs = dUs + DIM * NV * NSP * TE;        // [DIM][NV][NSP][TE]
   const OpTab<R> &op = optab<R>(a.vcjh, C::P);
   const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
   const Phys &ph = a.ph;
@@ -712,7 +722,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
     const S *dUg = static_cast<const S *>(a.dUg);
     for (int it = tid; it < DIM * NV * NS * TE; it += NT) {
       const int q = it / TE, e = it - q * TE, eg = e0 + e;
-      if (eg < a.nEle) dUs[it] = (R)dUg[(size_t)q * nE + eg];
+      if (eg < a.nEle) dUs[((q / NS) * NSP + sx<C>(q % NS)) * TE + e] = (R)dUg[(size_t)q * nE + eg];
     }
     __syncthreads();
   } else {
@@ -731,9 +741,9 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
     if (eg >= a.nEle) continue;
     R u[NV], g[DIM * NV];
 #pragma unroll
-    for (int v = 0; v < NV; v++) u[v] = Us[(v * NS + s) * TE + e];
+    for (int v = 0; v < NV; v++) u[v] = Us[(v * NSP + sx<C>(s)) * TE + e];
 #pragma unroll
-    for (int q = 0; q < DIM * NV; q++) g[q] = dUs[(q * NS + s) * TE + e];
+    for (int q = 0; q < DIM * NV; q++) g[q] = dUs[(q * NSP + sx<C>(s)) * TE + e];
     R Fi[DIM][NV], Fv[DIM][NV];
     inviscid_flux<DIM, NV, R>(u, Fi, ph);
     visc_flux<C, R>(u, g, Fv, ph);
@@ -753,7 +763,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
         R t = 0;
 #pragma unroll
         for (int d2 = 0; d2 < DIM; d2++) t += G[d1][d2] * Fv[d2][v];
-        Fs[((d1 * NV + v) * NS + s) * TE + e] = t;
+        Fs[((d1 * NV + v) * NSP + sx<C>(s)) * TE + e] = t;
       }
   }
   __syncthreads();
@@ -772,8 +782,8 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
 #pragma unroll
       for (int j = 0; j < N1; j++) {
         const R l = op.lag[side][j];
-        t += l * Us[(v * NS + s0 + j * st) * TE + e];
-        q += l * Fs[((dir * NV + v) * NS + s0 + j * st) * TE + e];
+        t += l * Us[(v * NSP + sx<C>(s0 + j * st)) * TE + e];
+        q += l * Fs[((dir * NV + v) * NSP + sx<C>(s0 + j * st)) * TE + e];
       }
       own[v] = t;
       dis[v] = side ? q : -q;
@@ -872,7 +882,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
 template <class C, typename R, typename S>
 __global__ void fr_trace_kernel(const double *__restrict__ U, S *__restrict__ tr, int nE, int nEle, int ldU,
                                 int vcjh) {
-  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1;
+  constexpr int NS = C::NS, NSP = C::NSP, NF = C::NF, NV = C::NV, N1 = C::N1;
   const OpTab<R> &op = optab<R>(vcjh, C::P);
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)NF * nE) return;
