@@ -660,6 +660,16 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
     if (dtn && prevE0 >= 0 && (tid >> 5) == NT / 32 - 1)
       dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, prevE0, tid & 31));
     if (NB == 2 && tid == 0) prefetch(j + 1, 0);
+    if (dtn) {
+      // the next tile's stored wave speeds and dA into L2, so its gathers
+      // (at its start) do not wait on DRAM
+      const int tn = blockIdx.x + (j + 1) * gridDim.x;
+      if (tn < nTiles)
+        for (int r = tid; r < 2 * NF; r += NT) {
+          const double *src = r < NF ? a.waveSp : a.dAd;
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(src + (size_t)(r % NF) * a.nE + (size_t)tn * TE));
+        }
+    }
     cp_async_wait_all();
     ok = mbar_wait(&bk[1], par);
     if (__syncthreads_or(!ok)) break;
@@ -878,6 +888,16 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
         issue_slot(slot(k ^ 1), tn * TE, &bar[3 * (k ^ 1)]);
         sIss++;
       }
+    }
+    if (dtn) {
+      // the next tile's stored wave speeds and dA into L2, so its gathers
+      // (at its start) do not wait on DRAM
+      const int tn = t + gridDim.x;
+      if (tn < nTiles)
+        for (int r = tid; r < 2 * NF; r += NT) {
+          const double *src = r < NF ? a.waveSp : a.dAd;
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(src + (size_t)(r % NF) * a.nE + (size_t)tn * TE));
+        }
     }
     cp_async_wait_all();
     ok = mbar_wait(&bk[1], par);
