@@ -899,6 +899,15 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
           asm volatile("prefetch.global.L2 [%0];" ::"l"(src + (size_t)(r % NF) * a.nE + (size_t)tn * TE));
         }
     }
+    if (nd.inU) {
+      // first stage: likewise the next tile's double input, whose bulk load
+      // is issued only once this tile's phase C has freed the buffer (the
+      // later stages gain nothing from it: measured)
+      const int tn = t + gridDim.x;
+      if (tn < nTiles)
+        for (int r = tid; r < NV * NS; r += NT)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.Uin_d + (size_t)r * a.ldU + (size_t)tn * TE));
+    }
     cp_async_wait_all();
     ok = mbar_wait(&bk[1], par);
     if (__syncthreads_or(!ok)) break;
