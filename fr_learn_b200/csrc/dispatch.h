@@ -34,7 +34,7 @@ struct KernelSet {
     // walking tiles with a stride of the grid size
     int persistent = 0, occ = 0;
   };
-  static constexpr int kMaxTma = 12;
+  static constexpr int kMaxTma = 16;
   TmaVariant tma[kMaxTma];
   int nTma = 0;
   int TE = 0;       // elements per block

@@ -23,6 +23,7 @@ void launch_stage_tma(const void *args, const void *maps, int nBlk, size_t smem,
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 cudaError_t add_tma_variant(KernelSet &k) {
   using TT = TileT<C, R, S, TEV, NTV>;
+  if (k.nTma >= KernelSet::kMaxTma) return cudaErrorInvalidValue;  // the variant table is full
   KernelSet::TmaVariant &v = k.tma[k.nTma++];
   v.launch = &launch_stage_tma<C, R, S, BC, RS, TEV, NTV>;
   v.TE = TT::TE;
@@ -42,6 +43,7 @@ void launch_stage_pipe(const void *args, const void *maps, int nBlk, size_t smem
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV, int NB>
 cudaError_t add_pipe_variant(KernelSet &k) {
   using TT = PipeT<C, R, S, TEV, NTV, NB>;
+  if (k.nTma >= KernelSet::kMaxTma) return cudaErrorInvalidValue;  // the variant table is full
   KernelSet::TmaVariant &v = k.tma[k.nTma++];
   v.launch = &launch_stage_pipe<C, R, S, BC, RS, TEV, NTV, NB>;
   v.TE = TT::TE;
@@ -64,6 +66,7 @@ void launch_stage_split(const void *args, const void *maps, int nBlk, size_t sme
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 cudaError_t add_split_variant(KernelSet &k) {
   using TT = SplitT<C, R, S, TEV, NTV>;
+  if (k.nTma >= KernelSet::kMaxTma) return cudaErrorInvalidValue;  // the variant table is full
   KernelSet::TmaVariant &v = k.tma[k.nTma++];
   v.launch = &launch_stage_split<C, R, S, BC, RS, TEV, NTV>;
   v.TE = TT::TE;

@@ -278,7 +278,7 @@ class Solver:
         `nsteps` steps of each candidate; the solution is left unchanged.
         Returns (chosen index, per-candidate ms per step)."""
         v = C.c_int()
-        out = np.zeros(12)  # FRG_MAX_TILE_VARIANTS
+        out = np.zeros(16)  # FRG_MAX_TILE_VARIANTS
         _check(lib().frg_autotune(self.h, nsteps, C.byref(v), out.ctypes.data))
         return v.value, out[:self.tile_variant_count()]
 

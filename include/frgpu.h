@@ -221,7 +221,7 @@ frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long
  * (frg_tile_variant_count entries, at most FRG_MAX_TILE_VARIANTS).  A no-op
  * where the TMA kernel is not used.  No counterpart in the reference, which
  * has a single CPU code path. */
-#define FRG_MAX_TILE_VARIANTS 12
+#define FRG_MAX_TILE_VARIANTS 16
 frg_status frg_autotune(frg_solver *s, int nsteps, int *variant_out, double *ms_out);
 /* Number of tile shapes the handle's configuration offers (1 without TMA). */
 frg_status frg_tile_variant_count(const frg_solver *s, int *count);
