@@ -239,6 +239,7 @@ def run_gpu(args, rank, world, local_rank):
     res["adjoint"] = run_adjoint_bump(stream)
     res["ensemble"] = run_ensemble(stream)
     res["tgv"] = run_tgv(stream, flush)
+    res["c1"] = run_advection_c1(stream)
     res["opgemm"] = run_operator_gemm(stream, flush)
     return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
 
@@ -515,6 +516,7 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
     mesh = tgv_mesh()
     out = {"workload": TGV_WORKLOAD}
     hist = {}
+    final = {}
     for name, prec in (("mixed", FRG_MIXED), ("fp64", FRG_FP64)):
         s = Solver(mesh, precision=prec, **tgv_params())
         s.set_stream(stream.cuda_stream)
@@ -548,6 +550,7 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
                 ke.append(kinetic_energy(s.get("U_spts"), detJ, TGV_P))
                 tt.append(s.time - t_start)
         hist[name] = (np.array(tt), np.array(ke))
+        final[name] = s.get("U_spts")
         b = bytes_per_dof_update(3, TGV_P, 5, 4 if prec == FRG_MIXED else 8, 4 if prec == FRG_MIXED else 8) / 4 * dof
         st_mean = float(np.mean(st[1:]))
         out[name] = {"value": dof / (ms * 1e-3), "ms_per_step": ms, "unit": "DOF-updates/s", "dof": dof,
@@ -557,6 +560,9 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
         s.set_stream(None)
         s.close()
     (tm, km), (td, kd) = hist["mixed"], hist["fp64"]
+    Um, Ud = final["mixed"], final["fp64"]
+    out["state_error_mixed_vs_fp64"] = {"steps": hist_steps, "rel_l2": float(np.linalg.norm(Um - Ud) / np.linalg.norm(Ud)),
+                                        "rel_linf": float(np.abs(Um - Ud).max() / np.abs(Ud).max())}
     eps_m = -np.gradient(km, tm)
     eps_d = -np.gradient(kd, td)
     out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
@@ -567,6 +573,60 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
         "dissipation_rate_max_rel_diff": float(np.max(np.abs(eps_m - eps_d)) / np.max(np.abs(eps_d))),
     }
     return out
+
+
+C1_WORKLOAD = "advection2d_gaussian_periodic_32x32_P3_upwind_rk44_dt1e-3_1000steps"
+
+
+def c1_mesh():
+    from fr_learn_b200 import box2d
+
+    return box2d(32, 32, -5.0, 5.0, -5.0, 5.0)
+
+
+def c1_params(**kw):
+    """Scalar advection at (1,1), Lax-Friedrichs flux with lambda 1 (upwind),
+    DG correction, RK4, fixed dt 1e-3 (FP64)."""
+    d = dict(order=3, equation=0, advectVx=1.0, advectVy=1.0, lambda_=1.0, timeType=4, dtType=0, dt=1e-3)
+    d.update(kw)
+    return d
+
+
+def run_advection_c1(stream, nsteps=1000):
+    """2D scalar advection of u0 = exp(-(x^2+y^2)) on the periodic square
+    [-5,5]^2, 32 x 32 linear quads, P = 3, FP64, 1000 RK4 steps of 1e-3:
+    DOF-updates/s over the run (CUDA events), and the relative L2 error at
+    t = 1 against the exact solution (the bump translated by (1,1))."""
+    import torch
+
+    from fr_learn_b200 import FRG_FP64, Solver
+
+    s = Solver(c1_mesh(), precision=FRG_FP64, **c1_params())
+    s.set_stream(stream.cuda_stream)
+    s.setInitialCondition(0)
+    with torch.cuda.stream(stream):
+        s.update(3)  # warm-up (graphs, kernels)
+        s.setInitialCondition(0)
+        s.setIter(0, 0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = s.time
+        a.record(stream)
+        s.update(nsteps)
+        b.record(stream)
+        b.synchronize()
+    ms = a.elapsed_time(b)
+    t = s.time - t0
+    pos, U = s.get("pos_spts"), s.get("U_spts")[..., 0]
+    x = np.mod(pos[..., 0] - t + 5.0, 10.0) - 5.0
+    y = np.mod(pos[..., 1] - t + 5.0, 10.0) - 5.0
+    ex = np.exp(-(x * x + y * y))
+    dof = s.nEles * s.nSpts * s.nFields
+    s.set_stream(None)
+    s.close()
+    return {"workload": C1_WORKLOAD, "dof": dof, "steps": nsteps, "time": t, "ms_per_step": ms / nsteps,
+            "value_fp64": dof * nsteps / (ms * 1e-3), "unit": "DOF-updates/s",
+            "rel_l2_vs_exact": float(np.linalg.norm(U - ex) / np.linalg.norm(ex)),
+            "note": "16,384 DOF: launch-latency bound (4 stage launches per step from one graph)"}
 
 
 def run_operator_gemm(stream, flush, reps=20):
@@ -747,6 +807,7 @@ def main():
         "adjoint": res["adjoint"],
         "ensemble": res["ensemble"],
         "taylor_green_3d": res["tgv"],
+        "advection_2d": res["c1"],
         "operator_gemm_tensor_cores": res["opgemm"],
         "gpu_launches": mixed["launches"],
         "clocks": clocks,

@@ -261,3 +261,17 @@ def test_tile_variants_identical_and_autotune_restores(precision, case):
     assert np.array_equal(s.get("U_spts"), U2) and s.time == t2 and s.dt == dt2
     s.update(2)
     assert np.array_equal(s.get("U_spts"), ref[0])
+
+
+def test_advection_config1_full_run(oracle):
+    """The first benchmark configuration in full: 2D scalar advection of a
+    Gaussian on the periodic square [-5,5]^2, 32 x 32 quads, P = 3, upwind
+    flux, RK4, dt 1e-3, 1000 steps, FP64 against the oracle."""
+    from fr_learn_b200 import box2d
+
+    mesh = box2d(32, 32, -5.0, 5.0, -5.0, 5.0)
+    g, o = pair(oracle, mesh, 0, order=3, equation=0, advectVx=1.0, advectVy=1.0, dt=1e-3)
+    g.update(1000)
+    o.update(1000)
+    assert relerr(g.get("U_spts"), o.U()) < FP64_TOL
+    assert abs(g.time - o.time) <= 1e-12 * o.time
