@@ -240,6 +240,7 @@ def run_gpu(args, rank, world, local_rank):
     res["ensemble"] = run_ensemble(stream)
     res["tgv"] = run_tgv(stream, flush)
     res["c1"] = run_advection_c1(stream)
+    res["scale"] = run_scale(stream, flush)
     res["opgemm"] = run_operator_gemm(stream, flush)
     return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
 
@@ -575,6 +576,47 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
     return out
 
 
+def run_scale(stream, flush, nx=512, steps=30):
+    """The headline workload's physics at production size: the same vortex
+    on 512 x 512 perturbed quads (262,144 elements, P = 4, 26.2 M DOF; a
+    mixed step moves ~5.6 GB, far beyond L2), mixed and FP64, each with its
+    autotuned tile variant; DOF-updates/s and the per-stage roofline
+    fraction."""
+    import torch
+
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver, box2d
+
+    mesh = box2d(nx, nx, -10.0, 10.0, -10.0, 10.0, perturb=0.1, seed=0)
+    out = {"workload": f"euler2d_isentropic_vortex_periodic_{nx}x{nx}_P4_roe_rk44_cfl0.5", "nEles": nx * nx}
+    for name, prec, sz in (("mixed", FRG_MIXED, 4), ("fp64", FRG_FP64, 8)):
+        s = Solver(mesh, precision=prec, **c2_params())
+        s.set_stream(stream.cuda_stream)
+        s.setInitialCondition(1)
+        with torch.cuda.stream(stream):
+            var = int(s.autotune(5)[0])
+            s.update(3)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            for k in range(steps):
+                flush.fill_(k & 0xFF)
+                ev[k][0].record(stream)
+                s.update(1)
+                ev[k][1].record(stream)
+            stream.synchronize()
+            st = s.time_stages(10, flush.data_ptr(), flush.numel()).tolist()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        dof = s.nEles * s.nSpts * s.nFields
+        b = bytes_per_dof_update(2, ORDER, 4, sz, sz) / 4 * dof
+        st_mean = float(np.mean(st[1:]))
+        out["dof"] = dof
+        out[name] = {"tile_variant": var, "value": dof / (ms * 1e-3), "ms_per_step": ms, "unit": "DOF-updates/s",
+                     "stage_ms": st_mean, "bytes_per_stage": b, "achieved_gbs": b / (st_mean * 1e-3) / 1e9,
+                     "hbm_frac": b / (st_mean * 1e-3) / 1e9 / peaks()[0]}
+        s.set_stream(None)
+        s.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 C1_WORKLOAD = "advection2d_gaussian_periodic_32x32_P3_upwind_rk44_dt1e-3_1000steps"
 
 
@@ -808,6 +850,7 @@ def main():
         "ensemble": res["ensemble"],
         "taylor_green_3d": res["tgv"],
         "advection_2d": res["c1"],
+        "euler2d_at_scale": res["scale"],
         "operator_gemm_tensor_cores": res["opgemm"],
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
