@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xc
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
 CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu",
-              "adjoint_2d.cu", "adjoint_3d.cu", "opgemm.cu"]
+              "adjoint_2d.cu", "adjoint_3d.cu", "opgemm.cu", "metrics.cu"]
 # The FP32 arithmetic of the mixed mode uses the hardware's approximate
 # single-precision divide and square root (within 2 ulp); FP64 arithmetic is
 # unaffected by these flags, so the FP64 units stay exact.

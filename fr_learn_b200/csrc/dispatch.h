@@ -79,6 +79,20 @@ size_t op_gemm_smem(int KP, int NP);
 cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
                            int nEle, int nV, float beta, unsigned *err, cudaStream_t st);
 
+// Element metrics on the device (metrics.cu), bitwise the host set-up's.
+// Device arrays in the handle's layout, rows of L elements; `pos` in the
+// reference layout [nS][nE][d].
+struct MetricOut {
+  double *pos, *detJd, *nrmOwn, *dAd, *vol;
+  void *JG, *detJs, *invDetS, *nrmC, *dAs;  // stored type (storeBytes)
+};
+// check != 0: only tests the solution-point Jacobians, flag[0] |= 1 and
+// flag[1] = min element when one is negative; else writes every metric.
+// xv [nE][nN][d]; tab = shS, dS, dF of MetricTables back to back.
+cudaError_t launch_metrics(int nDims, int storeBytes, const double *xv, const double *tab, const int *fdir,
+                           const int *fsgn, const double *wv, const int *nbr, int nN, int nS, int nF, int nE, int L,
+                           int check, const MetricOut &out, unsigned *flag, cudaStream_t st);
+
 // Uploads the 1D operator tables (all schemes, orders 0..5) into each unit.
 cudaError_t upload_tables_2d_f64();
 cudaError_t upload_tables_2d_f32();

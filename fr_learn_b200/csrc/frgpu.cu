@@ -250,6 +250,13 @@ struct frg_solver {
   AdjState *adj = nullptr;
   // frg_apply_operator: operator images for the tensor-core GEMM, [which][dim]
   float *opImg[5][3] = {};
+  // frg_update_geometry: node count, device copies of the nodes and of the
+  // shape tables, the check flags and the solution-point positions
+  int nNodes = 0;
+  double *xvDev = nullptr, *geoTab = nullptr, *posDev = nullptr;
+  int *geoInt = nullptr;
+  unsigned *geoFlag = nullptr;
+  bool waveStale = false;  // metrics changed: the next dt recomputes the wave speeds
 };
 
 namespace {
@@ -508,7 +515,7 @@ frg_status launch_group_step(frg_solver *s) {
 // dt work at the start of the next fused step (see frg_solver::graph).
 int dt_mode(const frg_solver *s) {
   if (s->p.dtType == 0) return 0;
-  if (s->iter == s->initIter + 1) return 2;
+  if (s->iter == s->initIter + 1 || s->waveStale) return 2;
   return (fused_dt(s) && s->dtFresh) ? 0 : 1;
 }
 
@@ -628,6 +635,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   frg_status st = build_geometry(p, *mesh, s->g, err);
   if (st) return fail(st, "%s", err.c_str());
   s->ops = build_ops1d(p.order, p.vcjhScheme);
+  s->nNodes = mesh->nNodes;
   s->nS = s->g.nS; s->nF = s->g.nF; s->nE = s->g.nE;
   s->L = (s->nE + 31) & ~31;
   if ((st = upload_tables(p.nDims, p.precision))) return st;
@@ -758,9 +766,60 @@ frg_status frg_destroy(frg_solver *s) {
   for (void *q : vp) if (q) cudaFree(q);
   for (auto &r : s->opImg)
     for (float *q : r) if (q) cudaFree(q);
+  void *gp[] = {s->xvDev, s->geoTab, s->posDev, s->geoInt, s->geoFlag};
+  for (void *q : gp) if (q) cudaFree(q);
   cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy
   if (own) cudaStreamDestroy(own);
   delete s;
+  return FRG_OK;
+}
+
+frg_status frg_update_geometry(frg_solver *s, const double *xv) {
+  if (!s || !xv) return fail(FRG_ERR_ARG, "null argument");
+  const int d = s->p.nDims, nN = s->nNodes, nS = s->nS, nF = s->nF, nE = s->nE, L = s->L;
+  const size_t nX = (size_t)nE * nN * d;
+  if (!s->geoTab) {
+    MetricTables t;
+    std::string err;
+    if (!metric_tables(d, s->p.order, s->p.vcjhScheme, nN, t, err)) return fail(FRG_ERR_ARG, "%s", err.c_str());
+    std::vector<double> tab(t.shS);
+    tab.insert(tab.end(), t.dS.begin(), t.dS.end());
+    tab.insert(tab.end(), t.dF.begin(), t.dF.end());
+    tab.insert(tab.end(), t.wv.begin(), t.wv.end());
+    std::vector<int> fi(t.fdir);
+    fi.insert(fi.end(), t.fsgn.begin(), t.fsgn.end());
+    CK(cudaMalloc(&s->geoTab, tab.size() * 8));
+    CK(cudaMemcpy(s->geoTab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&s->geoInt, fi.size() * sizeof(int)));
+    CK(cudaMemcpy(s->geoInt, fi.data(), fi.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&s->xvDev, nX * 8));
+    CK(cudaMalloc(&s->posDev, (size_t)nS * nE * d * 8));
+    CK(cudaMalloc(&s->geoFlag, 2 * sizeof(unsigned)));
+  }
+  const double *wv = s->geoTab + (size_t)nN * nS * (1 + d) + (size_t)nN * nF * d;
+  const int *fdir = s->geoInt, *fsgn = s->geoInt + nF;
+  CK(cudaMemcpyAsync(s->xvDev, xv, nX * 8, cudaMemcpyHostToDevice, s->stream));
+  const unsigned init[2] = {0u, 0xffffffffu};
+  CK(cudaMemcpyAsync(s->geoFlag, init, sizeof init, cudaMemcpyHostToDevice, s->stream));
+  MetricOut out{s->posDev, s->detJd, s->nrmOwn, s->dAd, s->vol, s->JG, s->detJs, s->invDetS, s->nrm, s->dAs};
+  // a negative Jacobian leaves the solver's metrics as they were
+  CK(launch_metrics(d, (int)s->sstore, s->xvDev, s->geoTab, fdir, fsgn, wv, s->nbr, nN, nS, nF, nE, L, 1, out,
+                    s->geoFlag, s->stream));
+  unsigned flag[2];
+  CK(cudaMemcpyAsync(flag, s->geoFlag, sizeof flag, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->launches += 1;
+  if (flag[0]) return fail(FRG_ERR_NEG_JAC, "Negative Jacobian at solution points (element %u)", flag[1]);
+  CK(launch_metrics(d, (int)s->sstore, s->xvDev, s->geoTab, fdir, fsgn, wv, s->nbr, nN, nS, nF, nE, L, 0, out,
+                    s->geoFlag, s->stream));
+  s->launches += 2;
+  // the host copies that frg_download serves
+  CK(cudaMemcpyAsync(s->g.pos_spts.data(), s->posDev, s->g.pos_spts.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpy2DAsync(s->g.detJ.data(), (size_t)nE * 8, s->detJd, (size_t)L * 8, (size_t)nE * 8, nS,
+                       cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->waveStale = true;
+  s->dtFresh = false;
   return FRG_OK;
 }
 
@@ -1042,9 +1101,10 @@ frg_status frg_calc_dt(frg_solver *s, double *dt_out) {
   if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: per-group dt via frg_update / frg_get_group_times");
   frg_status st;
   if (s->p.dtType != 0) {
-    if (s->iter == s->initIter + 1) {
+    if (s->iter == s->initIter + 1 || s->waveStale) {
       // calcWaveSpFpts reads U_fpts as the last extrapolation left it
       if ((st = ensure_traces(s)) || (st = launch_wavesp(s))) return st;
+      s->waveStale = false;
     }
     if ((st = launch_dt(s))) return st;
   }
@@ -1086,6 +1146,7 @@ static void step_done(frg_solver *s, int mode) {
   s->dtFresh = fused_dt(s);
   s->dtLast = s->dtCur;
   s->dtCur ^= (int)s->dtFresh;
+  if (mode == 2) s->waveStale = false;
 }
 
 frg_status frg_update(frg_solver *s, int nsteps) {
@@ -1332,7 +1393,9 @@ frg_status frg_time_stages(frg_solver *s, int nsteps, void *flush, unsigned long
   for (int n = 0; n < nsteps && !st; n++) {
     if (flush) CK(cudaMemsetAsync(flush, n & 0xff, flushBytes, s->stream));
     s->iter++;
-    st = enqueue_step(s, dt_mode(s), ev.data());
+    const int mode = dt_mode(s);
+    st = enqueue_step(s, mode, ev.data());
+    if (mode == 2) s->waveStale = false;
     s->dtFresh = fused_dt(s);
     s->dtLast = s->dtCur;
     s->dtCur ^= (int)s->dtFresh;

@@ -279,6 +279,48 @@ void dense_operator(int nDims, const Ops1D &o, int which, int dim, std::vector<d
   }
 }
 
+bool metric_tables(int d, int P, int vcjh, int nN, MetricTables &t, std::string &err) {
+  const int n1 = P + 1, nS = d == 2 ? n1 * n1 : n1 * n1 * n1, nFF = d == 2 ? n1 : n1 * n1, nF = 2 * d * nFF;
+  Shape sh;
+  if (!make_shape(d, nN, sh)) {
+    err = d == 3 ? "3D elements must be 8-node hexahedra" : "quad node count must be a square >= 4";
+    return false;
+  }
+  Ops1D o = build_ops1d(P, vcjh);
+  t.nDims = d; t.nS = nS; t.nF = nF; t.nN = nN;
+  t.shS.assign((size_t)nS * nN, 0.0);
+  t.dS.assign((size_t)d * nS * nN, 0.0);
+  t.dF.assign((size_t)d * nF * nN, 0.0);
+  for (int s = 0; s < nS; s++) {
+    double x[3];
+    loc_spt(d, o, s, x);
+    shape(sh, d, x, &t.shS[(size_t)s * nN]);
+    for (int dim = 0; dim < d; dim++) dshape(sh, d, x, dim, &t.dS[((size_t)dim * nS + s) * nN]);
+  }
+  t.fdir.resize(nF);
+  t.fsgn.resize(nF);
+  for (int f = 0; f < nF; f++) {
+    double x[3];
+    loc_fpt(d, o, f, x);
+    for (int dim = 0; dim < d; dim++) dshape(sh, d, x, dim, &t.dF[((size_t)dim * nF + f) * nN]);
+    FptLine L = fpt_line(d, P, f);
+    t.fdir[f] = L.dir;
+    t.fsgn[f] = L.side ? 1 : -1;
+  }
+  t.wv.resize(nS);
+  t.ws.resize(nF);
+  for (int s = 0; s < nS; s++) {
+    int i = s % n1, j = (s / n1) % n1, k = s / (n1 * n1);
+    // getQptWeights order: products w_slow * w_mid (* w_fast)
+    t.wv[s] = d == 2 ? o.w[j] * o.w[i] : o.w[k] * o.w[j] * o.w[i];
+  }
+  for (int f = 0; f < nF; f++) {
+    int k = f % nFF, a = k % n1, b = k / n1;
+    t.ws[f] = d == 2 ? o.w[k] : o.w[b] * o.w[a];
+  }
+  return true;
+}
+
 frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, std::string &err) {
   const int d = p.nDims, P = p.order, nE = m.nEles, n1 = P + 1;
   g.nDims = d; g.P = P; g.nE = nE;
@@ -287,25 +329,9 @@ frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, s
   g.nFaceEle = 2 * d;
   g.nF = g.nFaceEle * g.nFF;
   const int nS = g.nS, nF = g.nF, nN = m.nNodes;
-  Shape sh;
-  if (!make_shape(d, nN, sh)) {
-    err = d == 3 ? "3D elements must be 8-node hexahedra" : "quad node count must be a square >= 4";
-    return FRG_ERR_ARG;
-  }
-  Ops1D o = build_ops1d(P, p.vcjhScheme);
-  // shape data at spts / fpts
-  std::vector<double> shS((size_t)nS * nN), dS((size_t)d * nS * nN), dF((size_t)d * nF * nN);
-  for (int s = 0; s < nS; s++) {
-    double x[3];
-    loc_spt(d, o, s, x);
-    shape(sh, d, x, &shS[(size_t)s * nN]);
-    for (int dim = 0; dim < d; dim++) dshape(sh, d, x, dim, &dS[((size_t)dim * nS + s) * nN]);
-  }
-  for (int f = 0; f < nF; f++) {
-    double x[3];
-    loc_fpt(d, o, f, x);
-    for (int dim = 0; dim < d; dim++) dshape(sh, d, x, dim, &dF[((size_t)dim * nF + f) * nN]);
-  }
+  MetricTables t;
+  if (!metric_tables(d, P, p.vcjhScheme, nN, t, err)) return FRG_ERR_ARG;
+  const std::vector<double> &shS = t.shS, &dS = t.dS, &dF = t.dF, &wv = t.wv, &ws = t.ws;
   g.pos_spts.assign((size_t)nS * nE * d, 0.0);
   g.JG.assign((size_t)d * d * nS * nE, 0.0);
   g.detJ.assign((size_t)nS * nE, 0.0);
@@ -313,16 +339,6 @@ frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, s
   g.dA.assign((size_t)nF * nE, 0.0);
   g.vol.assign(nE, 0.0);
   g.dAw.assign((size_t)nF * nE, 0.0);
-  std::vector<double> wv(nS), ws(nF);
-  for (int s = 0; s < nS; s++) {
-    int i = s % n1, j = (s / n1) % n1, k = s / (n1 * n1);
-    // getQptWeights order: products w_slow * w_mid (* w_fast)
-    wv[s] = d == 2 ? o.w[j] * o.w[i] : o.w[k] * o.w[j] * o.w[i];
-  }
-  for (int f = 0; f < nF; f++) {
-    int k = f % g.nFF, a = k % n1, b = k / n1;
-    ws[f] = d == 2 ? o.w[k] : o.w[b] * o.w[a];
-  }
   auto X = [&](int e, int n, int k) { return m.xv[((size_t)e * nN + n) * d + k]; };
   // jacobian at a point from dshape rows: J[a][k] = d x_k / d xi_a
   auto jac = [&](const double *dsh, int nPt, int pt, int e, double J[3][3]) {
@@ -374,13 +390,12 @@ frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, s
       double J[3][3], G[3][3], det;
       jac(dF.data(), nF, f, e, J);
       adj(J, G, det);
-      FptLine L = fpt_line(d, P, f);
-      double tn = L.side ? 1.0 : -1.0;
+      const double tn = t.fsgn[f];
       double nv[3], mag = 0.0;
       // norm = JGinv^T tNorm: only the face-normal reference direction is non-zero
       for (int k = 0; k < d; k++) {
         nv[k] = 0.0;
-        for (int a = 0; a < d; a++) nv[k] += G[a][k] * (a == L.dir ? tn : 0.0);
+        for (int a = 0; a < d; a++) nv[k] += G[a][k] * (a == t.fdir[f] ? tn : 0.0);
       }
       for (int k = 0; k < d; k++) mag += nv[k] * nv[k];
       mag = sqrt(mag);

@@ -46,6 +46,21 @@ struct HostGeom {
   long nIntFaces = 0, nBndFaces = 0;
 };
 
+// Shape-function tables of the element metrics of one order and node count,
+// shared by the host set-up and the device metric kernel:
+//   shS [nS][nN]     node shape functions at the solution points
+//   dS  [d][nS][nN]  their reference derivatives at the solution points
+//   dF  [d][nF][nN]  ... and at the flux points
+//   fdir [nF]        normal reference direction of the flux point's face
+//   fsgn [nF]        +1 / -1 for the face at xi_dir = +1 / -1
+//   wv [nS], ws [nF] volume / surface quadrature weights
+struct MetricTables {
+  int nDims = 0, nS = 0, nF = 0, nN = 0;
+  std::vector<double> shS, dS, dF, wv, ws;
+  std::vector<int> fdir, fsgn;
+};
+bool metric_tables(int nDims, int P, int vcjh, int nNodes, MetricTables &t, std::string &err);
+
 // Builds metrics and connectivity.  Returns FRG_OK or an error with `err` set.
 frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, std::string &err);
 

@@ -86,6 +86,7 @@ def lib():
         "frg_create": ([C.POINTER(Params), C.POINTER(MeshC), C.POINTER(vp)], i),
         "frg_destroy": ([vp], i),
         "frg_info": ([vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)], i),
+        "frg_update_geometry": ([vp, vp], i),
         "frg_get_operator": ([vp, i, i, vp], i),
         "frg_apply_operator": ([vp, i, i, vp, vp, i, C.c_float], i),
         "frg_upload": ([vp, i, vp], i), "frg_download": ([vp, i, i, vp], i),
@@ -191,6 +192,13 @@ class Solver:
         """Y = Op X + beta Y on FP32 device arrays [nFields][points][ld] (the
         oper::apply* products as tensor-core GEMMs, see include/frgpu.h)."""
         _check(lib().frg_apply_operator(self.h, which, dim, X_ptr, Y_ptr, ld, beta))
+
+    def update_geometry(self, xv):
+        """Recomputes the metrics on the device for moved nodes xv
+        [nEles][nNodes][nDims] of the same mesh (solver::updateTransforms)."""
+        a = np.ascontiguousarray(xv, np.float64)
+        assert a.shape == np.shape(self.mesh.xv), (a.shape, np.shape(self.mesh.xv))
+        _check(lib().frg_update_geometry(self.h, a.ctypes.data))
 
     # -- the reference's entry points
     def setInitialCondition(self, icType=None, a0=0.0):

@@ -120,6 +120,20 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
 frg_status frg_inspect_geometry(const frg_params *params, const frg_mesh *mesh, int which, double *out,
                                 long *count);
 frg_status frg_destroy(frg_solver *s);
+
+/* Recomputes the element metrics on the device for new node coordinates of
+ * the same mesh (same elements, node count, connectivity and boundary
+ * conditions): solver::updateTransforms -> calcTransforms
+ * (src/solver.cpp:1358-1363, :1227-1356) and the solution-point positions
+ * of setPosSptsFpts (:904-951), for a mesh whose nodes moved.  xv is a host
+ * array [nEles][nNodes][nDims] as in frg_mesh.  The metrics are bitwise the
+ * ones frg_create builds on the host for those nodes.  The next CFL dt
+ * recomputes the wave speeds with the new normals.  Grid-velocity (ALE)
+ * flux terms are not part of this path.  FRG_ERR_NEG_JAC, with the solver's
+ * metrics unchanged, when a solution point has a negative Jacobian.
+ * Synchronises the solver's stream. */
+frg_status frg_update_geometry(frg_solver *s, const double *xv);
+
 frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, int *nEles);
 
 /* Dense operator matrices, row-major, as oper::setupOperators builds them:
