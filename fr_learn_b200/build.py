@@ -30,7 +30,7 @@ CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu
 # single-precision divide and square root (within 2 ulp); FP64 arithmetic is
 # unaffected by these flags, so the FP64 units stay exact.
 UNIT_FLAGS = {u: ["-prec-div=false", "-prec-sqrt=false"] for u in ("stage_2d_f32.cu", "stage_3d_f32.cu")}
-CXX_SOURCES = ["setup.cpp"]
+CXX_SOURCES = ["setup.cpp", "restart.cpp"]
 HEADERS = ["kernels.cuh", "kernels_tma.cuh", "adjoint.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
            "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
 

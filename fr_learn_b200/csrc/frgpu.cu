@@ -253,6 +253,7 @@ struct frg_solver {
   // frg_update_geometry: node count, device copies of the nodes and of the
   // shape tables, the check flags and the solution-point positions
   int nNodes = 0;
+  std::vector<double> xvHost;  // the current node coordinates (ParaView output)
   double *xvDev = nullptr, *geoTab = nullptr, *posDev = nullptr;
   int *geoInt = nullptr;
   unsigned *geoFlag = nullptr;
@@ -265,6 +266,13 @@ thread_local std::string g_err;
 // getCFLLimit (src/global.cpp:45-66)
 const double kCflLimit[6] = {1.393, 0.464, 0.235, 0.1453, 0.100, 0.0736};
 
+frg_status fail(frg_status st, const char *fmt, ...);
+}  // namespace
+namespace frg {
+// error reporting for the host-only units (restart.cpp)
+frg_status set_error(frg_status st, const std::string &msg) { return fail(st, "%s", msg.c_str()); }
+}  // namespace frg
+namespace {
 frg_status fail(frg_status st, const char *fmt, ...) {
   char buf[512];
   va_list ap;
@@ -636,6 +644,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
   if (st) return fail(st, "%s", err.c_str());
   s->ops = build_ops1d(p.order, p.vcjhScheme);
   s->nNodes = mesh->nNodes;
+  s->xvHost.assign(mesh->xv, mesh->xv + (size_t)mesh->nEles * mesh->nNodes * p.nDims);
   s->nS = s->g.nS; s->nF = s->g.nF; s->nE = s->g.nE;
   s->L = (s->nE + 31) & ~31;
   if ((st = upload_tables(p.nDims, p.precision))) return st;
@@ -818,9 +827,35 @@ frg_status frg_update_geometry(frg_solver *s, const double *xv) {
   CK(cudaMemcpy2DAsync(s->g.detJ.data(), (size_t)nE * 8, s->detJd, (size_t)L * 8, (size_t)nE * 8, nS,
                        cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(s->xvHost.data(), xv, nX * 8);
   s->waveStale = true;
   s->dtFresh = false;
   return FRG_OK;
+}
+
+frg_status frg_write_paraview(frg_solver *s, const char *dataFileName) {
+  if (!s || !dataFileName) return fail(FRG_ERR_ARG, "null argument");
+  if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: one time per case, write each case's solver");
+  std::vector<double> U((size_t)s->nS * s->nE * s->nV);
+  double t = 0.0;
+  frg_status st;
+  if ((st = frg_download(s, FRG_U_SPTS, 0, U.data())) || (st = frg_get_time(s, &t, nullptr, nullptr))) return st;
+  const frg_mesh m{s->nE, s->nNodes, s->xvHost.data(), nullptr, nullptr};
+  return frg_write_paraview_host(&s->p, &m, U.data(), t, s->iter, dataFileName);
+}
+
+frg_status frg_read_restart(frg_solver *s, const char *dataFileName, int restartIter) {
+  if (!s || !dataFileName) return fail(FRG_ERR_ARG, "null argument");
+  if (s->grp) return fail(FRG_ERR_ARG, "ensemble mode: restart each case's solver");
+  std::vector<double> U((size_t)s->nS * s->nE * s->nV);
+  double t = 0.0;
+  frg_status st;
+  if ((st = frg_read_restart_host(&s->p, s->nE, dataFileName, restartIter, U.data(), &t))) return st;
+  if ((st = frg_upload(s, FRG_U_SPTS, U.data()))) return st;
+  CK(cudaMemcpyAsync(s->timeDev, &t, 8, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  // input::readInputFile: initIter = restartIter (src/input.cpp:417-421)
+  return frg_set_iter(s, restartIter, restartIter);
 }
 
 frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, int *nEles) {

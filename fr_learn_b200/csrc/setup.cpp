@@ -321,6 +321,48 @@ bool metric_tables(int d, int P, int vcjh, int nN, MetricTables &t, std::string 
   return true;
 }
 
+bool plot_tables(int d, int P, int nN, std::vector<double> &shapeP, std::vector<double> &interpP, std::string &err) {
+  Shape sh;
+  if (!make_shape(d, nN, sh)) {
+    err = d == 3 ? "3D elements must be 8-node hexahedra" : "quad node count must be a square >= 4";
+    return false;
+  }
+  const Ops1D o = build_ops1d(P, 0);
+  const int n1 = P + 1, n3 = P + 3, nS = d == 2 ? n1 * n1 : n1 * n1 * n1, nP = d == 2 ? n3 * n3 : n3 * n3 * n3;
+  std::vector<double> x1(n3);
+  x1[0] = -1.0;
+  for (int i = 0; i < n1; i++) x1[i + 1] = o.pts[i];
+  x1[n3 - 1] = 1.0;
+  shapeP.assign((size_t)nP * nN, 0.0);
+  interpP.assign((size_t)nP * nS, 0.0);
+  for (int q = 0; q < nP; q++) {
+    const int i = q % n3, j = (q / n3) % n3, k = q / (n3 * n3);
+    const double loc[3] = {x1[i], x1[j], d == 3 ? x1[k] : 0.0};
+    shape(sh, d, loc, &shapeP[(size_t)q * nN]);
+    for (int s = 0; s < nS; s++) {
+      const int is = s % n1, js = (s / n1) % n1, ks = s / (n1 * n1);
+      double v = lagr(o.pts, n1, loc[0], is) * lagr(o.pts, n1, loc[1], js);
+      if (d == 3) v = v * lagr(o.pts, n1, loc[2], ks);
+      interpP[(size_t)q * nS + s] = v;
+    }
+  }
+  return true;
+}
+
+void order_interp(int d, int Pf, int Pt, std::vector<double> &out) {
+  const Ops1D of = build_ops1d(Pf, 0), ot = build_ops1d(Pt, 0);
+  const int nf = Pf + 1, nt = Pt + 1, nSf = d == 2 ? nf * nf : nf * nf * nf, nSt = d == 2 ? nt * nt : nt * nt * nt;
+  out.assign((size_t)nSt * nSf, 0.0);
+  for (int t = 0; t < nSt; t++) {
+    const double x = ot.pts[t % nt], y = ot.pts[(t / nt) % nt], z = d == 3 ? ot.pts[t / (nt * nt)] : 0.0;
+    for (int r = 0; r < nSf; r++) {
+      double v = lagr(of.pts, nf, x, r % nf) * lagr(of.pts, nf, y, (r / nf) % nf);
+      if (d == 3) v = v * lagr(of.pts, nf, z, r / (nf * nf));
+      out[(size_t)t * nSf + r] = v;
+    }
+  }
+}
+
 frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, std::string &err) {
   const int d = p.nDims, P = p.order, nE = m.nEles, n1 = P + 1;
   g.nDims = d; g.P = P; g.nE = nE;

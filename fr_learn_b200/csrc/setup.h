@@ -61,6 +61,17 @@ struct MetricTables {
 };
 bool metric_tables(int nDims, int P, int vcjh, int nNodes, MetricTables &t, std::string &err);
 
+// Plot points of the reference's ParaView / restart files: the tensor grid of
+// the 1D points {-1, solution points, +1}, x fastest (getLocPpts,
+// src/points.cpp:130-160), (P+3)^d per element.
+//   shapeP  [nP][nN]  node shape functions at the plot points
+//   interpP [nP][nS]  opp_spts_to_ppts (src/operators.cpp:114-140)
+bool plot_tables(int nDims, int P, int nNodes, std::vector<double> &shapeP, std::vector<double> &interpP,
+                 std::string &err);
+// Lagrange interpolation between the solution points of two orders
+// ([nS_to][nS_from], the restart's inter-order operator, src/ele.cpp:1506-1555).
+void order_interp(int nDims, int Pfrom, int Pto, std::vector<double> &out);
+
 // Builds metrics and connectivity.  Returns FRG_OK or an error with `err` set.
 frg_status build_geometry(const frg_params &p, const frg_mesh &m, HostGeom &g, std::string &err);
 

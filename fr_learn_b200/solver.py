@@ -87,6 +87,9 @@ def lib():
         "frg_destroy": ([vp], i),
         "frg_info": ([vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)], i),
         "frg_update_geometry": ([vp, vp], i),
+        "frg_write_paraview": ([vp, C.c_char_p], i), "frg_read_restart": ([vp, C.c_char_p, i], i),
+        "frg_write_paraview_host": ([C.POINTER(Params), C.POINTER(MeshC), vp, d, i, C.c_char_p], i),
+        "frg_read_restart_host": ([C.POINTER(Params), i, C.c_char_p, i, vp, C.POINTER(d)], i),
         "frg_get_operator": ([vp, i, i, vp], i),
         "frg_apply_operator": ([vp, i, i, vp, vp, i, C.c_float], i),
         "frg_upload": ([vp, i, vp], i), "frg_download": ([vp, i, i, vp], i),
@@ -199,6 +202,14 @@ class Solver:
         a = np.ascontiguousarray(xv, np.float64)
         assert a.shape == np.shape(self.mesh.xv), (a.shape, np.shape(self.mesh.xv))
         _check(lib().frg_update_geometry(self.h, a.ctypes.data))
+
+    def write_paraview(self, dataFileName):
+        """writeParaview: <dataFileName>_<iter:09d>.vtu of the current state."""
+        _check(lib().frg_write_paraview(self.h, os.fsencode(dataFileName)))
+
+    def read_restart(self, dataFileName, restartIter):
+        """readRestartFile: state and time from <dataFileName>_<restartIter:09d>.vtu."""
+        _check(lib().frg_read_restart(self.h, os.fsencode(dataFileName), restartIter))
 
     # -- the reference's entry points
     def setInitialCondition(self, icType=None, a0=0.0):
@@ -395,6 +406,31 @@ def inspect_geometry(mesh: Mesh, which: str, **params) -> np.ndarray:
     if which == "faces":
         return out.reshape(-1, 6).astype(np.int64)
     return out
+
+
+def write_paraview_host(mesh: Mesh, U, time, iter, dataFileName, **params):
+    """Host-only writeParaview of a state U [nSpts][nEles][nFields]."""
+    params.setdefault("nDims", mesh.nDims)
+    p = Params(**default_params(**params))
+    xv = np.ascontiguousarray(mesh.xv, np.float64)
+    m = MeshC(mesh.nEles, mesh.nNodes, xv.ctypes.data, None, None)
+    u = np.ascontiguousarray(U, np.float64)
+    _check(lib().frg_write_paraview_host(C.byref(p), C.byref(m), u.ctypes.data, float(time), int(iter),
+                                         os.fsencode(dataFileName)))
+
+
+def read_restart_host(nEles, dataFileName, restartIter, **params):
+    """Host-only restart read: (U [nSpts][nEles][nFields], time)."""
+    pd = default_params(**params)
+    p = Params(**pd)
+    n1 = pd["order"] + 1
+    nS = n1 ** pd["nDims"]
+    nV = 1 if pd["equation"] == 0 else pd["nDims"] + 2
+    U = np.empty((nS, nEles, nV), np.float64)
+    t = C.c_double(0.0)
+    _check(lib().frg_read_restart_host(C.byref(p), int(nEles), os.fsencode(dataFileName), int(restartIter),
+                                       U.ctypes.data, C.byref(t)))
+    return U, t.value
 
 
 class Ensemble:

@@ -134,6 +134,30 @@ frg_status frg_destroy(frg_solver *s);
  * Synchronises the solver's stream. */
 frg_status frg_update_geometry(frg_solver *s, const double *xv);
 
+/* The reference's ParaView file, which is also its restart file
+ * (writeParaview, src/output.cpp:103-391): <dataFileName>_<iter, 9 digits>.vtu
+ * with "<!-- TIME t -->" / "<!-- ITER n -->" header comments and per element
+ * one piece of (P+3)^d plot points (the 1D points {-1, solution points, +1}
+ * in a tensor grid, x fastest) carrying Density, Velocity and Pressure (the
+ * primitives interpolated from the solution points; Density alone for
+ * advection), their coordinates and the linear sub-cells, in ASCII with 16
+ * significant digits.  The reference writes 3D only; 2D files use the layout
+ * its restart reader expects, with a zero third velocity component.
+ * frg_write_paraview writes the solver's state at its iteration and time. */
+frg_status frg_write_paraview(frg_solver *s, const char *dataFileName);
+/* solver::readRestartFile / ele::restart (src/solver.cpp:1420-1482,
+ * src/ele.cpp:1451-1880): reads <dataFileName>_<restartIter, 9 digits>.vtu,
+ * takes the solution points' primitives (the interior plot points), converts
+ * them to conservative variables, interpolates from the file's order when it
+ * differs, and sets the state, the time (TIME comment) and iter = initIter =
+ * restartIter. */
+frg_status frg_read_restart(frg_solver *s, const char *dataFileName, int restartIter);
+/* Host-only forms (no device): U is [nSpts][nEles][nFields] as frg_download. */
+frg_status frg_write_paraview_host(const frg_params *params, const frg_mesh *mesh, const double *U, double time,
+                                   int iter, const char *dataFileName);
+frg_status frg_read_restart_host(const frg_params *params, int nEles, const char *dataFileName, int restartIter,
+                                 double *U, double *time);
+
 frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, int *nEles);
 
 /* Dense operator matrices, row-major, as oper::setupOperators builds them:

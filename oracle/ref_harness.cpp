@@ -22,6 +22,11 @@
  *         src/flurry.cpp:49-66, with dt and the L2 residual norm per step.
  *   time  <input> <nsteps>                  seconds per update() (setup and
  *         one warm-up step excluded), printed as one JSON line.
+ *   vtu   <input> <outdir> <nsteps>         <nsteps> update() calls, then
+ *         writeParaview (src/output.cpp:103) into <outdir>/ref_<iter>.vtu with
+ *         the state, nodes and time it wrote from; then a second solver
+ *         restarted from that file (readRestartFile, src/solver.cpp:1420) and
+ *         the state and time it read.
  *
  * Arrays are written as raw little-endian float64 / int32 files plus a
  * manifest (name dtype dims...) so numpy can read them.
@@ -42,6 +47,7 @@
 #include "input.hpp"
 #include "intFace.hpp"
 #include "operators.hpp"
+#include "output.hpp"
 #include "solver.hpp"
 
 static FILE *g_manifest = nullptr;
@@ -383,6 +389,50 @@ static int modeCase(char *inputFile, const char *out, int nsteps) {
   return 0;
 }
 
+static int modeVtu(char *inputFile, const char *out, int nsteps) {
+  openOut(out);
+  input params;
+  params.rank = 0;
+  params.nproc = 1;
+  params.readInputFile(inputFile);
+  solver S;
+  S.setup(&params, params.order);
+  S.initializeSolution();
+  params.iter = params.initIter;
+  for (int n = 0; n < nsteps; n++) {
+    params.iter++;
+    S.update();
+  }
+  const int nS = S.nSpts, nE = S.nEles, nD = S.nDims;
+  dumpArr("U_spts", S.U_spts, {nS, nE, (int)params.nFields});
+  dumpArr("nodes", S.nodes, {(int)S.nNodes, nE, nD});
+  double t = params.time;
+  dump("time", &t, 1, {1});
+  int it = params.iter;
+  dumpi("iter", &it, 1, {1});
+  params.dataFileName = std::string(out) + "/ref";
+  writeParaview(&S, &params);
+  /* restart a second solver from the file (input::readInputFile with
+     restart = 1 sets initIter = restartIter, src/input.cpp:417-421) */
+  input p2;
+  p2.rank = 0;
+  p2.nproc = 1;
+  p2.readInputFile(inputFile);
+  p2.restart = 1;
+  p2.restartIter = it;
+  p2.initIter = it;
+  p2.iter = it;
+  p2.dataFileName = params.dataFileName;
+  solver S2;
+  S2.setup(&p2, p2.order);
+  S2.initializeSolution();
+  dumpArr("restart_U_spts", S2.U_spts, {nS, nE, (int)p2.nFields});
+  double t2 = p2.time;
+  dump("restart_time", &t2, 1, {1});
+  fclose(g_manifest);
+  return 0;
+}
+
 static int modeTime(char *inputFile, int nsteps) {
   input params;
   params.rank = 0;
@@ -422,6 +472,7 @@ int main(int argc, char **argv) {
   if (mode == "kat" && argc == 3) return modeKat(argv[2]);
   if (mode == "case" && argc == 5) return modeCase(argv[2], argv[3], atoi(argv[4]));
   if (mode == "time" && argc == 4) return modeTime(argv[2], atoi(argv[3]));
+  if (mode == "vtu" && argc == 5) return modeVtu(argv[2], argv[3], atoi(argv[4]));
   fprintf(stderr, "bad arguments\n");
   return 2;
 }

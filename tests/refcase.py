@@ -98,6 +98,25 @@ def run_case(mesh, nsteps=0, workdir=None, **kw):
     return load(out)
 
 
+def run_vtu(mesh, nsteps=0, workdir=None, **kw):
+    """Run the harness 'vtu' mode: the dumped arrays plus the text of the
+    ParaView / restart file the reference wrote."""
+    if not os.path.exists(HARNESS):
+        build()
+    wd = workdir or tempfile.mkdtemp(prefix="frref_")
+    msh = os.path.join(wd, "mesh.msh")
+    bcnames = write_gmsh(mesh, msh)
+    inp = os.path.join(wd, "input.txt")
+    write_input(inp, msh, bcnames, **kw)
+    out = os.path.join(wd, "out")
+    subprocess.run([HARNESS, "vtu", inp, out, str(nsteps)], check=True, cwd=wd, stdout=subprocess.DEVNULL)
+    res = load(out)
+    it = int(res["iter"][0])
+    with open(os.path.join(out, f"ref_{it:09d}.vtu")) as f:
+        res["vtu"] = f.read()
+    return res
+
+
 def run_ops(nDims, order, vcjh=0):
     if not os.path.exists(HARNESS):
         build()
