@@ -1505,6 +1505,11 @@ struct AdjState {
   double *thetaDir = nullptr;  // 5 doubles, device
   double *ckpt = nullptr;    // (nCkpt + 1) states: U at steps 0, k, 2k, ... and U_N last
   double *stages = nullptr;  // k * nRK stage states of one segment
+  // checkpointed runs: a second set of stage slots, so that the reverse sweep
+  // recomputes segment c-1 on the side stream while it reverses segment c
+  double *stages2 = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   int ckptCap = 0, k = 0, nSteps = 0, stagesCap = 0;  // capacities in states / steps
   bool keepAll = false;  // the forward run kept every stage state
   // captured per-segment work of the reverse sweep, keyed by (kind, segment
@@ -1528,8 +1533,11 @@ void adj_free(frg_solver *s) {
   if (!a) return;
   for (auto &g : a->graphs) cudaGraphExecDestroy(g.second.exec);
   double *p[] = {a->seed[0], a->seed[1], a->lam[0], a->lam[1], a->trY, a->fnbar, a->ybar, a->grad, a->part,
-                 a->thetaBar, a->thetaDir, a->ckpt, a->stages};
+                 a->thetaBar, a->thetaDir, a->ckpt, a->stages, a->stages2};
   for (double *q : p) if (q) cudaFree(q);
+  if (a->evFork) cudaEventDestroy(a->evFork);
+  if (a->evJoin) cudaEventDestroy(a->evJoin);
+  if (a->side) cudaStreamDestroy(a->side);
   delete a;
   s->adj = nullptr;
 }
@@ -1575,7 +1583,11 @@ frg_status adj_init(frg_solver *s) {
     s->adj = a.release();
     return st;
   }
+  AdjState *ap = a.get();
   s->adj = a.release();
+  CK(cudaStreamCreateWithFlags(&ap->side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ap->evFork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ap->evJoin, cudaEventDisableTiming));
   return FRG_OK;
 }
 
@@ -1797,10 +1809,20 @@ frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery) {
     if ((st = dalloc(&a->ckpt, nSE * (nCkpt + 1)))) return st;
     a->ckptCap = nCkpt + 1;
   }
-  if (a->stages && a->stagesCap < k) { cudaFree(a->stages); a->stages = nullptr; }
+  if (a->stages && a->stagesCap < k) {
+    cudaFree(a->stages);
+    cudaFree(a->stages2);
+    a->stages = a->stages2 = nullptr;
+  }
   if (!a->stages) {
     if ((st = dalloc(&a->stages, nSE * (size_t)k * s->nRK))) return st;
     a->stagesCap = k;
+  }
+  // the overlap's second slot set; without the memory the sweep runs serially
+  if (!keepAll && nCkpt > 1 && !a->stages2 &&
+      cudaMalloc(&a->stages2, nSE * (size_t)a->stagesCap * s->nRK * 8) != cudaSuccess) {
+    cudaGetLastError();
+    a->stages2 = nullptr;
   }
   a->k = k;
   a->nSteps = nsteps;
@@ -1852,28 +1874,52 @@ frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const do
                                                  s->grp, s->grpDt);
   if ((st = post_launch(s))) return st;
   int cl = 0, cs = 0;  // current lam / seed buffers
-  double *seg = ad->stages;
+  // Checkpointed runs recompute segment c-1 from its checkpoint on the side
+  // stream while segment c is reversed on the solver's stream: the
+  // recomputation writes U, the RK accumulator, the traces and the other set
+  // of stage slots; the reversal reads only its own slots, the metrics and
+  // the adjoint buffers.  The solver's stream waits for the side stream
+  // before the next segment.  Without the second slot set: one after the other.
+  const bool overlap = !ad->keepAll && ad->stages2 && nCkpt > 1;
+  double *const bufs[2] = {ad->stages, overlap ? ad->stages2 : ad->stages};
+  const cudaStream_t mainSt = s->stream;
+  // recompute segment c into slot set b, keeping every stage state; one
+  // captured graph per segment length, trace-buffer parity and slot set
+  auto recompute = [&](int c, int b) -> frg_status {
+    const int m = std::min(k, N - c * k);
+    double *seg = bufs[b];
+    CK(cudaMemcpyAsync(s->U, ad->ckpt + nSE * c, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
+    s->trValid = false;
+    frg_status e = ensure_traces(s);
+    if (e) return e;
+    const int tr0 = s->curTr;
+    e = adj_replay(s, {2 * b, m, tr0, 0}, [&]() {
+      std::vector<double *> Y(nRK);
+      for (int j = 0; j < m; j++) {
+        for (int q = 0; q < nRK; q++) Y[q] = seg + nSE * ((size_t)j * nRK + q);
+        frg_status e2 = step_keep_stages(s, Y.data());
+        if (e2) return e2;
+      }
+      return FRG_OK;
+    });
+    if (e) return e;
+    s->curTr = tr0 ^ ((m * nRK) & 1);
+    return FRG_OK;
+  };
+  if (!ad->keepAll && (st = recompute(nCkpt - 1, 0))) return st;
+  int cur = 0;  // slot set holding the segment being reversed
   for (int c = nCkpt - 1; c >= 0; c--) {
     const int n0 = c * k, m = std::min(k, N - n0);
-    // recompute the segment from its checkpoint, keeping every stage state
-    // (already kept when the forward run stored them all); one captured
-    // graph per segment length and trace-buffer parity
-    if (!ad->keepAll) {
-      CK(cudaMemcpyAsync(s->U, ad->ckpt + nSE * c, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
-      s->trValid = false;
-      if ((st = ensure_traces(s))) return st;
-      const int tr0 = s->curTr;
-      st = adj_replay(s, {0, m, tr0, 0}, [&]() {
-        std::vector<double *> Y(nRK);
-        for (int j = 0; j < m; j++) {
-          for (int q = 0; q < nRK; q++) Y[q] = seg + nSE * ((size_t)j * nRK + q);
-          frg_status e = step_keep_stages(s, Y.data());
-          if (e) return e;
-        }
-        return FRG_OK;
-      });
+    double *seg = bufs[cur];
+    const bool fork = overlap && c > 0;
+    if (fork) {
+      CK(cudaEventRecord(ad->evFork, mainSt));
+      CK(cudaStreamWaitEvent(ad->side, ad->evFork, 0));
+      s->stream = ad->side;
+      st = recompute(c - 1, cur ^ 1);
+      s->stream = mainSt;
       if (st) return st;
-      s->curTr = tr0 ^ ((m * nRK) & 1);
+      CK(cudaEventRecord(ad->evJoin, ad->side));
     }
     // reverse the segment, stage by stage (captured when checkpointed: the
     // same slots serve every segment; a kept-all run is reversed once, launch
@@ -1899,10 +1945,16 @@ frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const do
       }
       return FRG_OK;
     };
-    st = ad->keepAll ? reverse() : adj_replay(s, {1, m, cl0, cs0}, reverse);
+    st = ad->keepAll ? reverse() : adj_replay(s, {1 + 2 * cur, m, cl0, cs0}, reverse);
     if (st) return st;
     cs = cs0 ^ ((m * nRK) & 1);
     cl = cl0 ^ (m & 1);
+    if (fork) {
+      CK(cudaStreamWaitEvent(mainSt, ad->evJoin, 0));
+      cur ^= 1;
+    } else if (!ad->keepAll && c > 0 && (st = recompute(c - 1, 0))) {
+      return st;
+    }
   }
   // the solution is the forward run's final state again
   CK(cudaMemcpyAsync(s->U, ad->ckpt + nSE * nCkpt, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));

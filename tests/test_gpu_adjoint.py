@@ -240,4 +240,7 @@ def test_checkpointed_and_stored_sweeps_agree():
         s.adjoint_forward(8, every)
         s.objective("wall_pressure")
         out.append(s.adjoint_backward(None, np.array([0.0, c, 0, 0, 0]))[0])
+        # a second sweep replays the captured segment graphs (both slot sets of
+        # the overlapped recompute / reverse) and must give the same bits
+        assert np.array_equal(s.adjoint_backward(None, np.array([0.0, c, 0, 0, 0]))[0], out[-1])
     assert relerr(out[1], out[0]) < 1e-12 and relerr(out[2], out[0]) < 1e-12
