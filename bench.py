@@ -23,7 +23,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -91,52 +90,96 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+    """SM clocks and throttle reasons of one GPU, sampled through NVML by a
+    background thread every ~10 ms from before the warm-up until after the
+    timed region.  `mark(True/False)` brackets the timed region; the summary
+    uses the samples taken inside it or, for a region shorter than the
+    sampling interval, the samples on either side of it."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index):
-        self.idx = gpu_index
-        self.proc = None
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.samples = []  # (time, sm MHz, reason bits)
+        self.windows = []
+        self.max_mhz = None
+        self.error = None
+
+    def _handle(self, nv):
+        import torch
+
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.idx).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:  # noqa: BLE001 -- fall back to the visible index
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip()]
+            phys = int(ids[self.idx]) if self.idx < len(ids) and ids[self.idx].strip().isdigit() else self.idx
+            return nv.nvmlDeviceGetHandleByIndex(phys)
 
     def __enter__(self):
+        import threading
+
+        self._stop = threading.Event()
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        except Exception as e:  # noqa: BLE001
+            self.error = f"NVML unavailable: {e}"
+            return self
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((time.perf_counter(), float(mhz), int(bits)))
+                except Exception as e:  # noqa: BLE001
+                    self.error = str(e)
+                    return
+                self._stop.wait(0.01)
+
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
+        time.sleep(0.05)
         return self
 
+    def mark(self, start):
+        if start:
+            self.windows.append([time.perf_counter(), None])
+        else:
+            self.windows[-1][1] = time.perf_counter()
+
     def __exit__(self, *a):
-        self.out = ""
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out = ""
+        self._stop.set()
+        if getattr(self, "_thread", None) is not None:
+            self._thread.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in (self.out or "").splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+        inside, near = [], []
+        for t0, t1 in self.windows:
+            if t1 is None:
                 continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+            w = [x for x in self.samples if t0 <= x[0] <= t1]
+            if w:
+                inside += w
+            else:
+                before = [x for x in self.samples if x[0] < t0][-1:]
+                after = [x for x in self.samples if x[0] > t1][:1]
+                near += before + after
+        use = inside or near
+        reasons = sorted({n for _, _, bits in use for n, b in self.REASONS if bits & b})
+        out = {"sm_mhz": statistics.median(x[1] for x in use) if use else None, "sm_max_mhz": self.max_mhz,
+               "reasons": reasons, "samples": len(use),
+               "source": "NVML every ~10 ms, " + ("inside the timed regions" if inside else
+                                                   "nearest samples around timed regions shorter than the interval")}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -161,21 +204,21 @@ def run_gpu(args, rank, world, local_rank):
             res.setdefault("tile_variant", {})[name] = int(s.autotune(10)[0])
         solvers[name] = s
     dof = solvers["mixed"].nEles * solvers["mixed"].nSpts * solvers["mixed"].nFields
-    clocks = None
-    for name, s in solvers.items():
-        with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
-                flush.fill_(1)
-                s.update(1)
-            stream.synchronize()
-            if world > 1:
-                torch.distributed.barrier()
-            torch.cuda.synchronize()
-            launches0 = s.launch_count()
-            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                  for _ in range(args.steps)]
-            sampler = ClockSampler(local_rank)
-            with sampler:
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        for name, s in solvers.items():
+            with torch.cuda.stream(stream):
+                for _ in range(args.warmup):
+                    flush.fill_(1)
+                    s.update(1)
+                stream.synchronize()
+                if world > 1:
+                    torch.distributed.barrier()
+                torch.cuda.synchronize()
+                launches0 = s.launch_count()
+                ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                      for _ in range(args.steps)]
+                sampler.mark(True)
                 t_wall = time.perf_counter()
                 for k in range(args.steps):
                     flush.fill_(k & 0xFF)
@@ -184,13 +227,15 @@ def run_gpu(args, rank, world, local_rank):
                     ev[k][1].record(stream)
                 stream.synchronize()
                 t_wall = time.perf_counter() - t_wall
-            torch.cuda.synchronize()
-            ms = sum(a.elapsed_time(b) for a, b in ev)
-            launches = s.launch_count() - launches0
-        ms = max_over_ranks(ms, world, dev)
-        res[name] ={"ms_total": ms, "ms_per_step": ms / args.steps, "launches": launches, "wall_s": t_wall}
-        if name == "mixed":
-            clocks = sampler.summary()
+                sampler.mark(False)
+                if world > 1:
+                    torch.distributed.barrier()
+                torch.cuda.synchronize()
+                ms = sum(a.elapsed_time(b) for a, b in ev)
+                launches = s.launch_count() - launches0
+            ms = max_over_ranks(ms, world, dev)
+            res[name] = {"ms_total": ms, "ms_per_step": ms / args.steps, "launches": launches, "wall_s": t_wall}
+    clocks = sampler.summary()
     # accuracy of the mixed path against the FP64 path after the same steps
     # (the FP64 path matches the FP64 oracle to 1e-12, see tests/)
     Um, Ud = solvers["mixed"].get("U_spts"), solvers["fp64"].get("U_spts")
@@ -772,14 +817,63 @@ def cpu_baseline(steps=2, threads=1):
     return dof * steps / dt, dt
 
 
+def profile_run(case, variant=None):
+    """A few steps of one workload and nothing else, for profiler captures
+    (`ncu ... python bench.py --profile CASE`): builds the handle, runs,
+    synchronises and returns.  Cases: c2_mixed / c2_fp64 (the 2D vortex
+    workload, 4 steps; `variant` picks the stage kernel's tile shape),
+    tgv_mixed / tgv_fp64 (3D Taylor-Green, 32^3 hexes, P = 3, 2 steps),
+    opgemm (the tensor-core operator GEMMs over the Taylor-Green arrays:
+    spts->fpts, grad_x, correction, 2 calls each)."""
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver
+
+    prec = FRG_FP64 if case.endswith("fp64") else FRG_MIXED
+    if case.startswith("c2"):
+        s = Solver(c2_mesh(), precision=prec, **c2_params())
+        s.setInitialCondition(1)
+        if variant is not None:
+            s.set_tile_variant(int(variant))
+        s.update(4)
+        s.sync()
+        print(case, "time", s.time)
+    elif case.startswith("tgv"):
+        s = Solver(tgv_mesh(), precision=prec, **tgv_params())
+        s.setInitialCondition(10, TGV_MA)
+        s.update(2)
+        s.sync()
+        print(case, "time", s.time)
+    elif case == "opgemm":
+        import torch
+
+        s = Solver(tgv_mesh(), precision=FRG_MIXED, **tgv_params())
+        s.set_stream(torch.cuda.current_stream().cuda_stream)
+        nV, nE, nS, nF = s.nFields, s.nEles, s.nSpts, s.nFpts
+        ld = (nE + 31) // 32 * 32
+        for which, (M, K) in ((0, (nF, nS)), (1, (nS, nS)), (3, (nS, nF))):
+            X = torch.randn((nV, K, ld), dtype=torch.float32, device="cuda")
+            Y = torch.empty((nV, M, ld), dtype=torch.float32, device="cuda")
+            for _ in range(2):
+                s.apply_operator(which, 0, X.data_ptr(), Y.data_ptr(), ld)
+            s.sync()
+            print(case, which, float(np.abs(Y.cpu().numpy()).max()))
+        s.set_stream(None)
+    else:
+        raise SystemExit(f"unknown profile case {case!r}")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile", nargs="+", metavar=("CASE", "VARIANT"),
+                    help="run a few steps of one workload for a profiler capture, then exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     args = ap.parse_args()
+    if args.profile:
+        return profile_run(args.profile[0], args.profile[1] if len(args.profile) > 1 else None)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

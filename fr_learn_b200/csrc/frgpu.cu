@@ -258,6 +258,9 @@ struct frg_solver {
   int *geoInt = nullptr;
   unsigned *geoFlag = nullptr;
   bool waveStale = false;  // metrics changed: the next dt recomputes the wave speeds
+  // frg_calc_residual_noalloc on a caller's stream: recorded on the handle's
+  // stream so the caller's stream waits for pending uploads / geometry work
+  cudaEvent_t noallocOrder = nullptr;
 };
 
 namespace {
@@ -608,6 +611,10 @@ frg_status unfused_update(frg_solver *s);
 
 }  // namespace
 
+// Device address of the allocation-free residual's scratch array on the
+// current device (defined next to the array, below).
+static frg_status noalloc_scratch_addr(void **out);
+
 // ==================================================================== C ABI
 extern "C" {
 
@@ -718,6 +725,14 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     s->useTma = !(env && std::strcmp(env, "generic") == 0);
     if (s->useTma && (st = setup_tma(s.get()))) return st;
   }
+  CK(cudaEventCreateWithFlags(&s->noallocOrder, cudaEventDisableTiming));
+  {
+    // the allocation-free residual's scratch address on this device, looked
+    // up here so that the module holding it is resident before any
+    // frg_calc_residual_noalloc call
+    void *scratch = nullptr;
+    if ((st = noalloc_scratch_addr(&scratch))) return st;
+  }
   CK(cudaDeviceSynchronize());
   *out = s.release();
   return FRG_OK;
@@ -777,6 +792,7 @@ frg_status frg_destroy(frg_solver *s) {
     for (float *q : r) if (q) cudaFree(q);
   void *gp[] = {s->xvDev, s->geoTab, s->posDev, s->geoInt, s->geoFlag};
   for (void *q : gp) if (q) cudaFree(q);
+  if (s->noallocOrder) cudaEventDestroy(s->noallocOrder);
   cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy
   if (own) cudaStreamDestroy(own);
   delete s;
@@ -1025,6 +1041,26 @@ void *g_noalloc_addr[kMaxDevices] = {nullptr};
 std::mutex g_noalloc_mu;
 }  // namespace
 
+// Set-up once per device, with that device current: the array's device
+// address by cudaGetSymbolAddress (the host-side symbol is not a device
+// pointer).  frg_create calls this, so the lookup and the loading of this
+// module happen there, not inside the allocation-free call.
+static frg_status noalloc_scratch_addr(void **out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(FRG_ERR_ARG, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(FRG_ERR_CUDA, "cudaGetSymbolAddress(noalloc scratch): %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return FRG_OK;
+}
+
 extern "C" {
 
 frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double *divF_dev, void *stream) {
@@ -1036,23 +1072,16 @@ frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double 
   if (need > kNoAllocScratchBytes)
     return fail(FRG_ERR_ARG, "frg_calc_residual_noalloc: traces need %zu bytes, the scratch array holds %zu", need,
                 kNoAllocScratchBytes);
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return fail(FRG_ERR_ARG, "device index %d out of range", dev);
   void *scratch = nullptr;
-  {
-    // set-up once per device, with that device current
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      void *p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p)
-        return fail(FRG_ERR_CUDA, "cudaGetSymbolAddress(noalloc scratch): %s", cudaGetErrorString(e));
-      g_noalloc_addr[dev] = p;
-    }
-    scratch = g_noalloc_addr[dev];
-  }
+  frg_status sst = noalloc_scratch_addr(&scratch);  // looked up by frg_create on this device already
+  if (sst) return sst;
   cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+  if (st != s->stream) {
+    // after the work pending on the handle's stream (uploads, geometry
+    // updates) that wrote the metrics this residual reads
+    CK(cudaEventRecord(s->noallocOrder, s->stream));
+    CK(cudaStreamWaitEvent(st, s->noallocOrder, 0));
+  }
   // traces of the caller's state into the scratch array, then the residual
   s->ks.trace(U_dev, scratch, s->L, s->nE, s->nE, s->p.vcjhScheme, st);
   CK(cudaGetLastError());
@@ -1195,6 +1224,10 @@ frg_status frg_update(frg_solver *s, int nsteps) {
       if ((st = unfused_update(s))) return st;
     return check_flags(s);
   }
+  // writeResidual's check (src/output.cpp:823-824); a CFL dt is checked on
+  // the device where it is computed
+  if (nsteps > 0 && s->p.dtType == 0 && !s->grp && !(s->p.dt >= 1e-13))
+    return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
   if ((st = ensure_traces(s))) return st;
   for (int n = 0; n < nsteps; n++) {
     s->iter++;

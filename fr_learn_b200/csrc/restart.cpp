@@ -227,9 +227,13 @@ frg_status frg_read_restart_host(const frg_params *params, int nEles, const char
         break;
       }
     if (!piece) {
-      char m[96];
-      snprintf(m, sizeof m, "restart file has fewer elements (%d) than the mesh (%d)", e, nE);
-      return set_error(FRG_ERR_ARG, m);
+      // ele::restart (src/ele.cpp:1469-1478): an element the file does not
+      // hold is reported and its solution set to 100 in every field; the
+      // read goes on with the next element
+      printf("Restart-file element doesn't exist!\n");
+      for (int s = 0; s < nS; s++)
+        for (int k = 0; k < nV; k++) U[((size_t)s * nE + e) * nV + k] = 100.;
+      continue;
     }
     const long nPts = atol(attr(line, "NumberOfPoints").c_str()), nCells = atol(attr(line, "NumberOfCells").c_str());
     // nCells = (order + 2)^d sub-cells

@@ -115,6 +115,12 @@ bool make_set(KernelSet &k, std::string &err) {
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess) {
+    // load the trace kernel now (lazy module loading would otherwise load it
+    // at its first launch, e.g. inside frg_calc_residual_noalloc)
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, fr_trace_kernel<C, R, S>);
+  }
   if constexpr (C::DIM == 2) {
     // variant 0 is the default; the others are candidates for frg_autotune
     k.nTma = 0;
@@ -155,6 +161,10 @@ bool make_set_visc(KernelSet &k, std::string &err) {
     e = cudaFuncSetAttribute(f1, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(f2, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess) {
+    cudaFuncAttributes fa;  // load the trace kernel now (see make_set)
+    e = cudaFuncGetAttributes(&fa, fr_trace_kernel<C, R, S>);
+  }
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;
 }

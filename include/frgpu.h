@@ -150,7 +150,8 @@ frg_status frg_write_paraview(frg_solver *s, const char *dataFileName);
  * takes the solution points' primitives (the interior plot points), converts
  * them to conservative variables, interpolates from the file's order when it
  * differs, and sets the state, the time (TIME comment) and iter = initIter =
- * restartIter. */
+ * restartIter.  As in ele::restart (src/ele.cpp:1469-1478), an element the
+ * file has no piece for is reported on stdout and set to 100 in every field. */
 frg_status frg_read_restart(frg_solver *s, const char *dataFileName, int restartIter);
 /* Host-only forms (no device): U is [nSpts][nEles][nFields] as frg_download. */
 frg_status frg_write_paraview_host(const frg_params *params, const frg_mesh *mesh, const double *U, double time,
@@ -216,10 +217,15 @@ frg_status frg_calc_dt(frg_solver *s, double *dt_out);
  * device memory that the library declares statically: every GPU that loads
  * the library keeps it until the process exits.  Meshes whose traces
  * (nFields * nFpts * nEles values, 8 bytes each in FP64 mode, 4 in mixed
- * mode) exceed 16 MiB are rejected with FRG_ERR_ARG.  The first call on a
- * device looks up the scratch array's device address (no allocation); make
- * that first call before any stream capture.  All calls share the one scratch
- * array and it keeps the last call's contents; every value a call reads is
+ * mode; viscous runs add one or two more arrays of that size for the
+ * projected viscous fluxes) exceed 16 MiB are rejected with FRG_ERR_ARG.
+ * frg_create does the set-up on its device: it looks up the scratch array's
+ * device address (cudaGetSymbolAddress) and loads the kernels this call
+ * launches, so the call itself only launches kernels.  On a stream other
+ * than the handle's, the call first makes that stream wait (an event the
+ * handle owns) for the work pending on the handle's stream, such as an
+ * upload or a frg_update_geometry.  All calls share the one scratch array
+ * and it keeps the last call's contents; every value a call reads is
  * written by the same call first, so nothing needs clearing.  Calls that
  * overlap on the GPU (different streams, or several handles at once) race on
  * the scratch array: serialise them. */

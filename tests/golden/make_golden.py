@@ -1,6 +1,6 @@
 """Generates tests/golden/reference_golden.npz from the FlurryPP reference itself.
 
-Run in a checkout that has the reference sources at /root/reference:
+Run where the reference sources are present, at $REFDIR (default /root/reference):
 
     python tests/golden/make_golden.py
 

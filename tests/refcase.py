@@ -16,14 +16,16 @@ HARNESS = os.path.join(ROOT, "oracle", "_ref", "refharness")
 BCNAME = {1: "char", 2: "sup_in", 3: "sup_out", 4: "sub_in", 5: "sub_out", 8: "slip_wall",
           9: "isothermal_noslip", 10: "adiabatic_noslip"}
 HEXFV = ((0, 1, 2, 3), (4, 5, 6, 7), (3, 0, 4, 7), (2, 1, 5, 6), (1, 0, 4, 5), (3, 2, 6, 7))
+# the reference checkout whose sources oracle/Makefile compiles
+REFDIR = os.environ.get("REFDIR", "/root/reference")
 
 
 def available() -> bool:
-    return os.path.isdir("/root/reference/src")
+    return os.path.isdir(os.path.join(REFDIR, "src"))
 
 
 def build():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REFDIR={REFDIR}"], check=True)
 
 
 def load(outdir):

@@ -144,10 +144,13 @@ def test_residual_norm(oracle):
     assert relerr(g.getNormResidual(2), o.residual_norm(2)) < FP64_TOL
 
 
+MIXED_L2_TOL = 1e-6  # relative L2 of the mixed path against the FP64 oracle
+
+
 def test_mixed_precision_bound(oracle):
     """Mixed mode (FP32 operators, fluxes, traces, metrics; FP64 Riemann
-    pressure and RK accumulation) stays within 1e-5 relative of the FP64
-    oracle over 20 RK4 steps of the perturbed-mesh vortex."""
+    pressure and RK accumulation) stays within 1e-6 relative L2 (1e-5 max
+    norm) of the FP64 oracle over 20 RK4 steps of the perturbed-mesh vortex."""
     from fr_learn_b200 import FRG_MIXED, box2d
 
     mesh = box2d(8, 8, -10, 10, -10, 10, perturb=0.1, seed=7)
@@ -156,8 +159,25 @@ def test_mixed_precision_bound(oracle):
     o.update(20)
     U, R = g.get("U_spts"), o.U()
     l2 = np.linalg.norm(U - R) / np.linalg.norm(R)
-    assert l2 < 1e-5, l2
+    assert l2 < MIXED_L2_TOL, l2
     assert relerr(U, R) < 1e-5
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_precision_bound_every_case(oracle, name):
+    """The mixed-mode bound on every parity case (2D / 3D, inviscid and
+    viscous, periodic and walled): 5 RK4 steps within 1e-6 relative L2 of the
+    FP64 oracle."""
+    from fr_learn_b200 import FRG_MIXED
+
+    mesh, ic, kw = cases()[name]
+    a0 = 0.1 if ic == 10 else 0.0
+    g, o = pair(oracle, mesh, ic, a0, precision=FRG_MIXED, **kw)
+    g.update(5)
+    o.update(5)
+    U, R = g.get("U_spts"), o.U()
+    l2 = np.linalg.norm(U - R) / np.linalg.norm(R)
+    assert l2 < MIXED_L2_TOL, l2
 
 
 def test_operators_match_oracle(oracle):

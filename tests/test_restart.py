@@ -100,10 +100,24 @@ def test_reader_errors(tmp_path):
     mesh = box2d(3, 3)
     U = _state(9, mesh.nEles, 4, 0)
     write_paraview_host(mesh, U, 0.0, 1, base, nDims=2, order=2)
-    with pytest.raises(FrgError, match="fewer elements"):
-        read_restart_host(mesh.nEles + 1, base, 1, nDims=2, order=2)
     path = f"{base}_{1:09d}.vtu"
     text = open(path).read().replace('Name="Pressure"', 'Name="Other"')
     open(path, "w").write(text)
     with pytest.raises(FrgError, match="missing"):
         read_restart_host(mesh.nEles, base, 1, nDims=2, order=2)
+
+
+def test_short_file_fills_missing_elements(tmp_path, capfd):
+    """A file with fewer pieces than the mesh has elements: like ele::restart
+    (src/ele.cpp:1469-1478) the reader reports each missing element, sets
+    its solution to 100 in every field and reads on; the elements the file
+    holds are restored as usual."""
+    base = str(tmp_path / "short")
+    mesh = box2d(3, 3)
+    U = _state(9, mesh.nEles, 4, 0)
+    write_paraview_host(mesh, U, 0.5, 1, base, nDims=2, order=2)
+    U2, t = read_restart_host(mesh.nEles + 2, base, 1, nDims=2, order=2)
+    assert t == 0.5
+    assert np.abs(U2[:, :mesh.nEles] - U).max() <= 1e-14 * np.abs(U).max()
+    assert np.all(U2[:, mesh.nEles:] == 100.0)
+    assert capfd.readouterr().out.count("Restart-file element doesn't exist!") == 2
