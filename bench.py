@@ -51,13 +51,17 @@ def c2_params(**kw):
     return d
 
 
-def bytes_per_dof_update(nDims, P, nV, s, g):
+def bytes_per_dof_update(nDims, P, nV, s, g, viscous=False):
     """Algorithmic bytes per DOF-update (4 RK stages), the per-element model:
-    nS*nV*(2s+24) + nS*(d^2+1)*g + nF*(d+1)*g + 4*nF*nV*s + 4*nF per stage."""
+    nS*nV*(2s+24) + nS*(d^2+1)*g + nF*(d+1)*g + 4*nF*nV*s + 4*nF per stage,
+    plus (2+2d)*nF*nV*s for a viscous stage (the common-solution and gradient
+    traces)."""
     n1 = P + 1
     nS = n1 ** nDims
     nF = 2 * nDims * n1 ** (nDims - 1)
     per_stage = nS * nV * (2 * s + 24) + nS * (nDims * nDims + 1) * g + nF * (nDims + 1) * g + 4 * nF * nV * s + 4 * nF
+    if viscous:
+        per_stage += (2 + 2 * nDims) * nF * nV * s
     return 4 * per_stage / (nS * nV)
 
 
@@ -597,7 +601,8 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
                 tt.append(s.time - t_start)
         hist[name] = (np.array(tt), np.array(ke))
         final[name] = s.get("U_spts")
-        b = bytes_per_dof_update(3, TGV_P, 5, 4 if prec == FRG_MIXED else 8, 4 if prec == FRG_MIXED else 8) / 4 * dof
+        b = bytes_per_dof_update(3, TGV_P, 5, 4 if prec == FRG_MIXED else 8, 4 if prec == FRG_MIXED else 8,
+                                 viscous=True) / 4 * dof
         st_mean = float(np.mean(st[1:]))
         out[name] = {"value": dof / (ms * 1e-3), "ms_per_step": ms, "unit": "DOF-updates/s", "dof": dof,
                      "launches_per_step": launches, "stage_ms": st_mean, "bytes_per_stage": b,
@@ -962,6 +967,8 @@ def main():
         "fp64_density_rel_l2_vs_exact_vortex": errs[2],
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic_source": "static: dram__bytes_read.sum + dram__bytes_write.sum of one stage launch "
+                                       "from the committed ncu capture (profiles/), not measured in this run",
                      "kernel": ("fr_stage_tma_split_kernel" if tiles["mixed"] >= 10 else "fr_stage_tma_pipe_kernel"
                                 if tiles["mixed"] >= 6 else "fr_stage_tma_kernel")
                                + f" (mixed, tile variant {tiles['mixed']})", "launch_ms": st_mixed,

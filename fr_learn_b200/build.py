@@ -24,14 +24,14 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC"] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
-CU_SOURCES = ["frgpu.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu",
+CU_SOURCES = ["frgpu.cu", "integrals.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", "stage_3d_f64.cu", "stage_3d_f32.cu",
               "adjoint_2d.cu", "adjoint_3d.cu", "opgemm.cu", "metrics.cu"]
 # The FP32 arithmetic of the mixed mode uses the hardware's approximate
 # single-precision divide and square root (within 2 ulp); FP64 arithmetic is
 # unaffected by these flags, so the FP64 units stay exact.
 UNIT_FLAGS = {u: ["-prec-div=false", "-prec-sqrt=false"] for u in ("stage_2d_f32.cu", "stage_3d_f32.cu")}
-CXX_SOURCES = ["setup.cpp", "restart.cpp"]
-HEADERS = ["kernels.cuh", "kernels_tma.cuh", "adjoint.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
+CXX_SOURCES = ["setup.cpp", "restart.cpp", "gmsh.cpp"]
+HEADERS = ["kernels.cuh", "kernels_tma.cuh", "kernels_visc_tma.cuh", "adjoint.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
            "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
 
 

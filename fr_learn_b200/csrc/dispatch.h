@@ -40,6 +40,13 @@ struct KernelSet {
   int TE = 0;       // elements per block
   int NT = 0;       // threads per block
   size_t smem = 0;  // dynamic shared memory per block
+  // 3D viscous configurations: the fused update's two passes with TMA tile
+  // movement (gradient / projected viscous flux, then the stage); `maps`
+  // points at a ViscMaps built for tiles of vTE elements
+  void (*vgrad)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
+  void (*vstage)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
+  int vTE = 0;
+  size_t vgradSmem = 0, vstageSmem = 0;
 };
 
 struct KernelKey {
@@ -92,6 +99,41 @@ struct MetricOut {
 cudaError_t launch_metrics(int nDims, int storeBytes, const double *xv, const double *tab, const int *fdir,
                            const int *fsgn, const double *wv, const int *nbr, int nN, int nS, int nF, int nE, int L,
                            int check, const MetricOut &out, unsigned *flag, cudaStream_t st);
+
+// Output integrals on the device (integrals.cu).  Boundary integrals of the
+// current traces: kind 0 computeWallForce (6 sums: pressure, viscous), kind
+// 1..3 computeMassFlux with errorNorm kind - 1 (nV sums); six partial sums per
+// block (boundary_integral_blocks blocks).
+struct BndIntArgs {
+  int kind, nDims, nV, P, nF, nFF, nS, nE, L, viscous;
+  const void *tr;     // traces [nV][nF][L], stored type
+  const void *dUg;    // corrected gradient at the solution points [d][nV][nS][L] (viscous), stored type
+  const int *nbr;     // [nF][L]
+  const double *nrm;  // the element's own unit normal [d][nF][L]
+  const double *dA;   // [nF][L]
+  const double *w1;   // 1D Gauss weights [P+1] (device)
+  double lag[2][6];   // 1D Lagrange basis at xi = -1 / +1
+  Phys ph;
+};
+int boundary_integral_blocks(int nF, int L);
+cudaError_t launch_boundary_integral(const BndIntArgs &a, int storeBytes, double *part, cudaStream_t st);
+// integrateError: per (quadrature point, element), 2 nV partial sums per block
+// (error_integral_blocks blocks): the error and the state, times weight and
+// detJ.
+struct ErrIntArgs {
+  int nDims, nV, nS, nQ, nE, L, nN, icType, errorNorm;
+  const double *U;       // [nV][nS][L]
+  const double *detJ;    // [nS][L]
+  const double *xv;      // [nE][nN][d] node coordinates
+  const double *interp;  // [nQ][nS] solution points -> quadrature points, or null (nQ = nS)
+  const double *shape;   // [nQ][nN] node shape functions at the quadrature points
+  const double *wq;      // [nQ] quadrature weights
+  double box[4];         // xmin, xmax, ymin, ymax of the analytic solution's period
+  double time, eps;
+  Phys ph;
+};
+int error_integral_blocks(int nQ, int nE);
+cudaError_t launch_error_integral(const ErrIntArgs &a, double *part, cudaStream_t st);
 
 // Uploads the 1D operator tables (all schemes, orders 0..5) into each unit.
 cudaError_t upload_tables_2d_f64();

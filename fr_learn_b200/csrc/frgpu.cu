@@ -19,6 +19,7 @@
 #include "dispatch.h"
 #include "kernels.cuh"
 #include "kernels_tma.cuh"
+#include "kernels_visc_tma.cuh"
 #include "adjoint.cuh"
 #include "setup.h"
 
@@ -58,8 +59,9 @@ __global__ void __launch_bounds__(256) fr_dt_kernel(const double *__restrict__ w
       my = dte;
       if (grp) {  // ensemble mode: the minimum per group (dtOut preset to a huge value)
         if (!(dte > 1e-13)) atomicOr(err, ERRF_DT);
-        else atomicMin(reinterpret_cast<unsigned long long *>(dtOut + grp[e]),
-                       (unsigned long long)__double_as_longlong(dte));
+        if (dte > 0)  // a tiny dt is still used, as the reference does before its check
+          atomicMin(reinterpret_cast<unsigned long long *>(dtOut + grp[e]),
+                    (unsigned long long)__double_as_longlong(dte));
       }
     }
     if (grp) return;
@@ -247,6 +249,12 @@ struct frg_solver {
   int tmaVar = 0;  // tile-shape variant of the TMA kernel (frg_autotune)
   int nBlkTma = 0;
   CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
+  // tensor maps of the 3D viscous TMA passes (tiles of ks.vTE elements):
+  // stage inputs W[i] in the padded point layout, and the rest
+  bool useViscTma = false;
+  struct {
+    CUtensorMap Win[2], U, Acc, Wout[2], tr[2], JG, det, nrm, dA, nbr, fvn, fvn2;
+  } vm;
   AdjState *adj = nullptr;
   // frg_apply_operator: operator images for the tensor-core GEMM, [which][dim]
   float *opImg[5][3] = {};
@@ -261,6 +269,12 @@ struct frg_solver {
   // frg_calc_residual_noalloc on a caller's stream: recorded on the handle's
   // stream so the caller's stream waits for pending uploads / geometry work
   cudaEvent_t noallocOrder = nullptr;
+  // output integrals (frg_wall_force, frg_mass_flux, frg_integrate_error):
+  // per-block partial sums, the 1D Gauss weights and the quadrature tables
+  // of the last quadOrder used
+  double *intPart = nullptr, *w1Dev = nullptr, *qShape = nullptr, *qInterp = nullptr, *qW = nullptr;
+  size_t intPartCap = 0;
+  int qOrder = -2;  // quadOrder of the cached tables (-1: the solution points)
 };
 
 namespace {
@@ -446,6 +460,70 @@ frg_status make_map(CUtensorMap *m, void *base, CUtensorMapDataType dt, int esz,
   return FRG_OK;
 }
 
+// Tensor map of `rank` dimensions: dims in elements (innermost first),
+// strides in bytes of dimensions 1..rank-1, box extents.
+frg_status make_map_nd(CUtensorMap *m, void *base, CUtensorMapDataType dt, int esz, int rank, const cuuint64_t *dims,
+                       const cuuint64_t *strides, const cuuint32_t *box) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if (((size_t)box[0] * esz) % 16 || ((uintptr_t)base & 15)) return fail(FRG_ERR_ARG, "tensor map not TMA-compatible");
+  for (int i = 0; i < rank; i++)
+    if (box[i] < 1 || box[i] > 256) return fail(FRG_ERR_ARG, "tensor map box extent out of range");
+  for (int i = 0; i < rank - 1; i++)
+    if (strides[i] % 16) return fail(FRG_ERR_ARG, "tensor map stride not a multiple of 16 bytes");
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(m, dt, (cuuint32_t)rank, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return FRG_OK;
+}
+
+// Maps of the 3D viscous TMA passes (kernels_visc_tma.cuh, ViscMaps).
+frg_status setup_visc_tma(frg_solver *s) {
+  const int TE = s->ks.vTE, d = s->p.nDims, n1 = s->p.order + 1, nS = s->nS, nF = s->nF, nV = s->nV;
+  const cuuint64_t L = (cuuint64_t)s->L;
+  const int es = (int)s->sstore;
+  const CUtensorMapDataType ts = es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint32_t te = (cuuint32_t)TE;
+  auto map3 = [&](CUtensorMap *m, void *base, CUtensorMapDataType dt, int esz, int rows, int planes) {
+    const cuuint64_t dims[3] = {L, (cuuint64_t)rows, (cuuint64_t)planes};
+    const cuuint64_t str[2] = {L * esz, L * esz * rows};
+    const cuuint32_t box[3] = {te, (cuuint32_t)rows, (cuuint32_t)planes};
+    return make_map_nd(m, base, dt, esz, 3, dims, str, box);
+  };
+  auto map2 = [&](CUtensorMap *m, void *base, CUtensorMapDataType dt, int esz, int rows) {
+    const cuuint64_t dims[2] = {L, (cuuint64_t)rows};
+    const cuuint64_t str[1] = {L * esz};
+    const cuuint32_t box[2] = {te, (cuuint32_t)rows};
+    return make_map_nd(m, base, dt, esz, 2, dims, str, box);
+  };
+  // stage input in the padded point layout: the xi line walked with a box one
+  // point wider than the line (the extra point is outside the tensor: zeros)
+  auto map_padded = [&](CUtensorMap *m, void *base) {
+    const cuuint64_t dims[4] = {L, (cuuint64_t)n1, (cuuint64_t)(nS / n1), (cuuint64_t)nV};
+    const cuuint64_t str[3] = {L * es, L * es * n1, L * es * nS};
+    const cuuint32_t box[4] = {te, (cuuint32_t)(n1 + 1), (cuuint32_t)(nS / n1), (cuuint32_t)nV};
+    return make_map_nd(m, base, ts, es, 4, dims, str, box);
+  };
+  const CUtensorMapDataType f64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  frg_status st;
+  if ((st = map_padded(&s->vm.Win[0], s->W[0])) || (st = map_padded(&s->vm.Win[1], s->W[1])) ||
+      (st = map3(&s->vm.U, s->U, f64, 8, nS, nV)) || (st = map3(&s->vm.Acc, s->Acc, f64, 8, nS, nV)) ||
+      (st = map3(&s->vm.Wout[0], s->W[0], ts, es, nS, nV)) || (st = map3(&s->vm.Wout[1], s->W[1], ts, es, nS, nV)) ||
+      (st = map3(&s->vm.tr[0], s->tr[0], ts, es, nF, nV)) || (st = map3(&s->vm.tr[1], s->tr[1], ts, es, nF, nV)) ||
+      (st = map3(&s->vm.JG, s->JG, ts, es, nS, d * d)) || (st = map2(&s->vm.det, s->invDetS, ts, es, nS)) ||
+      (st = map3(&s->vm.nrm, s->nrm, ts, es, nF, d)) || (st = map2(&s->vm.dA, s->dAs, ts, es, nF)) ||
+      (st = map3(&s->vm.fvn, s->fvn, ts, es, nF, nV)) ||
+      (st = map3(&s->vm.fvn2, s->visc2 ? s->fvn2 : s->fvn, ts, es, nF, nV)))
+    return st;
+  if (TE * 4 >= 16) {
+    if ((st = map2(&s->vm.nbr, s->nbr, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, nF))) return st;
+  } else {
+    s->vm.nbr = s->vm.det;  // codes read by plain loads; the map is not used
+  }
+  return FRG_OK;
+}
+
 frg_status setup_tma(frg_solver *s) {
   const int TE = s->ks.tma[s->tmaVar].TE, L = s->L, d = s->p.nDims;
   const CUtensorMapDataType ts = s->sstore == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -567,7 +645,26 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       a.divF = s->divF[0];
     }
     if (last && fused_dt(s)) a.flags |= SF_DTNEXT;
-    if (s->useTma) {
+    if (s->useViscTma) {
+      ViscMaps vm;
+      vm.Uin = first ? s->vm.U : s->vm.Win[(k - 1) & 1];
+      vm.U = s->vm.U;
+      vm.Acc = s->vm.Acc;
+      vm.Wout = s->vm.Wout[k & 1];
+      vm.trOut = s->vm.tr[s->curTr ^ 1];
+      vm.JG = s->vm.JG;
+      vm.det = s->vm.det;
+      vm.nrm = s->vm.nrm;
+      vm.dA = s->vm.dA;
+      vm.nbr = s->vm.nbr;
+      vm.fvn = s->vm.fvn;
+      vm.fvn2 = s->vm.fvn2;
+      const int nBlk = (s->nE + s->ks.vTE - 1) / s->ks.vTE;
+      s->ks.vgrad(&a, &vm, nBlk, s->ks.vgradSmem, s->stream);
+      if ((st = post_launch(s))) return st;
+      s->ks.vstage(&a, &vm, nBlk, s->ks.vstageSmem, s->stream);
+      st = post_launch(s);
+    } else if (s->useTma) {
       TmaMaps mm;
       mm.U = s->mU;
       mm.Acc = s->mAcc;
@@ -599,8 +696,9 @@ frg_status check_flags(frg_solver *s) {
   CK(cudaStreamSynchronize(s->stream));
   if (h) {
     CK(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->stream));
-    if (h & ERRF_NAN) return fail(FRG_ERR_NAN, "NaN encountered in the solution");
+    // writeResidual's order: the dt check first (src/output.cpp:823-824), then NaN
     if (h & ERRF_DT) return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
+    if (h & ERRF_NAN) return fail(FRG_ERR_NAN, "NaN encountered in the solution");
     if (h & ERRF_BC) return fail(FRG_ERR_ARG, "Boundary condition not recognized");
     if (h & ERRF_TIMEOUT) return fail(FRG_ERR_TIMEOUT, "a bounded device wait gave up");
   }
@@ -725,6 +823,11 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     s->useTma = !(env && std::strcmp(env, "generic") == 0);
     if (s->useTma && (st = setup_tma(s.get()))) return st;
   }
+  if (s->ks.vgrad) {
+    const char *env = getenv("FRG_KERNEL");
+    s->useViscTma = !(env && std::strcmp(env, "generic") == 0);
+    if (s->useViscTma && (st = setup_visc_tma(s.get()))) return st;
+  }
   CK(cudaEventCreateWithFlags(&s->noallocOrder, cudaEventDisableTiming));
   {
     // the allocation-free residual's scratch address on this device, looked
@@ -790,6 +893,8 @@ frg_status frg_destroy(frg_solver *s) {
   for (void *q : vp) if (q) cudaFree(q);
   for (auto &r : s->opImg)
     for (float *q : r) if (q) cudaFree(q);
+  void *ip[] = {s->intPart, s->w1Dev, s->qShape, s->qInterp, s->qW};
+  for (void *q : ip) if (q) cudaFree(q);
   void *gp[] = {s->xvDev, s->geoTab, s->posDev, s->geoInt, s->geoFlag};
   for (void *q : gp) if (q) cudaFree(q);
   if (s->noallocOrder) cudaEventDestroy(s->noallocOrder);
@@ -1773,6 +1878,166 @@ frg_status adj_check_path(const frg_solver *s) {
 }  // namespace
 
 extern "C" {
+
+}  // extern "C"
+
+namespace {
+// Partial-sum buffer of at least n doubles.
+frg_status int_part(frg_solver *s, size_t n) {
+  if (s->intPartCap >= n) return FRG_OK;
+  if (s->intPart) CK(cudaFree(s->intPart));
+  s->intPart = nullptr;
+  CK(cudaMalloc(&s->intPart, n * 8));
+  s->intPartCap = n;
+  return FRG_OK;
+}
+// Sum of nOut components over nb blocks of partials, in block order.
+frg_status sum_parts(frg_solver *s, int nb, int stride, int nOut, double *out) {
+  std::vector<double> h((size_t)nb * stride);
+  CK(cudaMemcpyAsync(h.data(), s->intPart, h.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (int j = 0; j < nOut; j++) {
+    double t = 0;
+    for (int b = 0; b < nb; b++) t += h[(size_t)b * stride + j];
+    out[j] = t;
+  }
+  return FRG_OK;
+}
+// Traces of the current state and, for viscous runs, its corrected gradient
+// at the solution points (what calcResidual(0) leaves in U_fpts / dU_spts).
+frg_status boundary_inputs(frg_solver *s, BndIntArgs &b, int kind) {
+  frg_status st;
+  s->trValid = false;
+  if ((st = ensure_traces(s))) return st;
+  if (s->p.viscous) {
+    StageArgs a = base_args(s);
+    a.Uin_d = s->U;
+    a.trIn = s->tr[s->curTr];
+    a.dUg = s->dUg;
+    a.flags = SF_RESIDUAL;
+    s->ks.grad(&a, s->nBlk, s->ks.smem, s->stream);
+    if ((st = post_launch(s))) return st;
+  }
+  if (!s->w1Dev) {
+    CK(cudaMalloc(&s->w1Dev, 8 * (MAXP + 1)));
+    CK(cudaMemcpy(s->w1Dev, s->ops.w, 8 * (MAXP + 1), cudaMemcpyHostToDevice));
+  }
+  b = BndIntArgs{};
+  b.kind = kind;
+  b.nDims = s->p.nDims;
+  b.nV = s->nV;
+  b.P = s->p.order;
+  b.nF = s->nF;
+  b.nFF = s->g.nFF;
+  b.nS = s->nS;
+  b.nE = s->nE;
+  b.L = s->L;
+  b.viscous = s->p.viscous;
+  b.tr = s->tr[s->curTr];
+  b.dUg = s->dUg;
+  b.nbr = s->nbr;
+  b.nrm = s->nrmOwn;
+  b.dA = s->dAd;
+  b.w1 = s->w1Dev;
+  for (int side = 0; side < 2; side++)
+    for (int j = 0; j <= MAXP; j++) b.lag[side][j] = s->ops.lag[side][j];
+  b.ph = make_phys(s->p);
+  return int_part(s, (size_t)boundary_integral_blocks(s->nF, s->L) * 6);
+}
+}  // namespace
+
+extern "C" {
+
+frg_status frg_wall_force(frg_solver *s, double *force) {
+  if (!s || !force) return fail(FRG_ERR_ARG, "null argument");
+  if (s->p.equation != 1) {
+    for (int j = 0; j < 6; j++) force[j] = 0;
+    return FRG_OK;
+  }
+  BndIntArgs b;
+  frg_status st = boundary_inputs(s, b, 0);
+  if (st) return st;
+  CK(launch_boundary_integral(b, (int)s->sstore, s->intPart, s->stream));
+  s->launches++;
+  return sum_parts(s, boundary_integral_blocks(s->nF, s->L), 6, 6, force);
+}
+
+frg_status frg_mass_flux(frg_solver *s, int errorNorm, double *flux) {
+  if (!s || !flux || errorNorm < 0 || errorNorm > 2) return fail(FRG_ERR_ARG, "bad arguments");
+  BndIntArgs b;
+  frg_status st = boundary_inputs(s, b, errorNorm + 1);
+  if (st) return st;
+  CK(launch_boundary_integral(b, (int)s->sstore, s->intPart, s->stream));
+  s->launches++;
+  return sum_parts(s, boundary_integral_blocks(s->nF, s->L), 6, s->nV, flux);
+}
+
+frg_status frg_integrate_error(frg_solver *s, int icType, double eps, int errorNorm, int quadOrder,
+                               const double *box, double *err) {
+  if (!s || !box || !err || errorNorm < 0 || errorNorm > 2) return fail(FRG_ERR_ARG, "bad arguments");
+  const bool ns = s->p.equation == 1;
+  if ((ns && icType != 0 && icType != 1) || (!ns && (icType < 0 || icType > 2)))
+    return fail(FRG_ERR_ARG, "integrateError: icType %d has no analytic solution here", icType);
+  const int d = s->p.nDims, nN = s->nNodes;
+  // the node coordinates on the device (kept current by frg_update_geometry)
+  if (!s->xvDev) {
+    const size_t nX = (size_t)s->nE * nN * d;
+    CK(cudaMalloc(&s->xvDev, nX * 8));
+    CK(cudaMemcpy(s->xvDev, s->xvHost.data(), nX * 8, cudaMemcpyHostToDevice));
+  }
+  const int want = errorNorm == 0 ? -1 : quadOrder;
+  int nQ = s->nS;
+  if (s->qOrder != want) {
+    std::vector<double> shp, itp, wq;
+    std::string e;
+    bool ok = want < 0 ? spt_shape_table(d, s->p.order, nN, shp, e)
+                       : quad_tables(d, s->p.order, nN, quadOrder, shp, itp, wq, e);
+    if (!ok) return fail(FRG_ERR_ARG, "%s", e.c_str());
+    for (double **q : {&s->qShape, &s->qInterp, &s->qW})
+      if (*q) { CK(cudaFree(*q)); *q = nullptr; }
+    frg_status st;
+    if ((st = upload_d(&s->qShape, shp))) return st;
+    if (want >= 0 && ((st = upload_d(&s->qInterp, itp)) || (st = upload_d(&s->qW, wq)))) return st;
+    s->qOrder = want;
+  }
+  if (want >= 0) nQ = d == 2 ? (quadOrder + 1) * (quadOrder + 1) : (quadOrder + 1) * (quadOrder + 1) * (quadOrder + 1);
+  ErrIntArgs a{};
+  a.nDims = d;
+  a.nV = s->nV;
+  a.nS = s->nS;
+  a.nQ = nQ;
+  a.nE = s->nE;
+  a.L = s->L;
+  a.nN = nN;
+  a.icType = icType;
+  a.errorNorm = errorNorm;
+  a.U = s->U;
+  a.detJ = s->detJd;
+  a.xv = s->xvDev;
+  a.interp = want >= 0 ? s->qInterp : nullptr;
+  a.shape = s->qShape;
+  a.wq = want >= 0 ? s->qW : s->wvol;
+  for (int j = 0; j < 4; j++) a.box[j] = box[j];
+  double t, dt;
+  int it;
+  frg_get_time(s, &t, &dt, &it);
+  a.time = t;
+  a.eps = eps;
+  a.ph = make_phys(s->p);
+  const int nb = error_integral_blocks(nQ, s->nE);
+  frg_status st = int_part(s, (size_t)nb * 2 * s->nV);
+  if (st) return st;
+  CK(launch_error_integral(a, s->intPart, s->stream));
+  s->launches++;
+  std::vector<double> r(2 * s->nV);
+  if ((st = sum_parts(s, nb, 2 * s->nV, 2 * s->nV, r.data()))) return st;
+  for (int k = 0; k < s->nV; k++) {
+    if (errorNorm == 0) err[k] = std::fabs(r[k] - r[s->nV + k]);
+    else if (errorNorm == 2) err[k] = std::sqrt(std::fabs(r[k]));
+    else err[k] = r[k];
+  }
+  return FRG_OK;
+}
 
 frg_status frg_objective(frg_solver *s, int kind, double *J, double *grad_host) {
   if (!s || !J) return fail(FRG_ERR_ARG, "null argument");

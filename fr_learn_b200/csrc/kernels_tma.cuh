@@ -416,8 +416,9 @@ __device__ __forceinline__ double tma_tile_dt(const StageArgs &a, const double *
   a.eleDt[eg] = dte;
   if (a.grp) {  // ensemble mode: each element into its own group's minimum
     if (!(dte > 1e-13)) atomicOr(a.err, ERRF_DT);
-    else atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext + a.grp[eg]),
-                   (unsigned long long)__double_as_longlong(dte));
+    if (dte > 0)  // a tiny dt is still used, as the reference does before its check
+      atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext + a.grp[eg]),
+                (unsigned long long)__double_as_longlong(dte));
   }
   return dte;
 }
@@ -432,7 +433,8 @@ __device__ __forceinline__ void tma_dt_reduce(const StageArgs &a, double my) {
   }
   if ((threadIdx.x & 31) == 0 && !a.grp) {
     if (!(my > 1e-13)) atomicOr(a.err, ERRF_DT);  // also catches NaN
-    else atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext), (unsigned long long)__double_as_longlong(my));
+    if (my > 0)  // a tiny dt is still used, as the reference does before its check
+      atomicMin(reinterpret_cast<unsigned long long *>(a.dtNext), (unsigned long long)__double_as_longlong(my));
   }
 }
 

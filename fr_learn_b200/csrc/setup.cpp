@@ -349,6 +349,91 @@ bool plot_tables(int d, int P, int nN, std::vector<double> &shapeP, std::vector<
   return true;
 }
 
+// Gauss-Legendre nodes (ascending) and weights of n points by Newton's
+// method on the Legendre polynomial; the reference tabulates them to 16
+// digits (src/points.cpp:169-248, :376-470), which agree to rounding.
+static void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w) {
+  const double pi = 3.141592653589793;
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    double z = -std::cos(pi * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; k++) {
+        const double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    double p0 = 1.0, p1 = z;
+    for (int k = 2; k <= n; k++) {
+      const double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    dp = n * (z * p1 - p0) / (z * z - 1.0);
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+bool quad_tables(int d, int P, int nN, int quadOrder, std::vector<double> &shapeQ, std::vector<double> &interpQ,
+                 std::vector<double> &wq, std::string &err) {
+  Shape sh;
+  if (!make_shape(d, nN, sh)) {
+    err = d == 3 ? "3D elements must be 8-node hexahedra" : "quad node count must be a square >= 4";
+    return false;
+  }
+  if (quadOrder < 0 || quadOrder > 20) {
+    err = "quadOrder out of range (0..20)";
+    return false;
+  }
+  const Ops1D o = build_ops1d(P, 0);
+  const int n1 = P + 1, nq = quadOrder + 1, nS = d == 2 ? n1 * n1 : n1 * n1 * n1;
+  const int nQ = d == 2 ? nq * nq : nq * nq * nq;
+  std::vector<double> xq, w1;
+  gauss_legendre(nq, xq, w1);
+  shapeQ.assign((size_t)nQ * nN, 0.0);
+  interpQ.assign((size_t)nQ * nS, 0.0);
+  wq.assign(nQ, 0.0);
+  for (int q = 0; q < nQ; q++) {
+    const int i = q % nq, j = (q / nq) % nq, k = q / (nq * nq);
+    const double loc[3] = {xq[i], xq[j], d == 3 ? xq[k] : 0.0};
+    // getQptWeights: the slowest index's weight first
+    wq[q] = d == 2 ? w1[j] * w1[i] : w1[k] * w1[j] * w1[i];
+    shape(sh, d, loc, &shapeQ[(size_t)q * nN]);
+    for (int s = 0; s < nS; s++) {
+      const int is = s % n1, js = (s / n1) % n1, ks = s / (n1 * n1);
+      double v = lagr(o.pts, n1, loc[0], is) * lagr(o.pts, n1, loc[1], js);
+      if (d == 3) v = v * lagr(o.pts, n1, loc[2], ks);
+      interpQ[(size_t)q * nS + s] = v;
+    }
+  }
+  return true;
+}
+
+bool spt_shape_table(int d, int P, int nN, std::vector<double> &shapeS, std::string &err) {
+  Shape sh;
+  if (!make_shape(d, nN, sh)) {
+    err = d == 3 ? "3D elements must be 8-node hexahedra" : "quad node count must be a square >= 4";
+    return false;
+  }
+  const Ops1D o = build_ops1d(P, 0);
+  const int nS = d == 2 ? (P + 1) * (P + 1) : (P + 1) * (P + 1) * (P + 1);
+  shapeS.assign((size_t)nS * nN, 0.0);
+  for (int s = 0; s < nS; s++) {
+    double loc[3] = {0, 0, 0};
+    loc_spt(d, o, s, loc);
+    shape(sh, d, loc, &shapeS[(size_t)s * nN]);
+  }
+  return true;
+}
+
 void order_interp(int d, int Pf, int Pt, std::vector<double> &out) {
   const Ops1D of = build_ops1d(Pf, 0), ot = build_ops1d(Pt, 0);
   const int nf = Pf + 1, nt = Pt + 1, nSf = d == 2 ? nf * nf : nf * nf * nf, nSt = d == 2 ? nt * nt : nt * nt * nt;

@@ -68,6 +68,14 @@ bool metric_tables(int nDims, int P, int vcjh, int nNodes, MetricTables &t, std:
 //   interpP [nP][nS]  opp_spts_to_ppts (src/operators.cpp:114-140)
 bool plot_tables(int nDims, int P, int nNodes, std::vector<double> &shapeP, std::vector<double> &interpP,
                  std::string &err);
+// Gauss points of quadOrder (the reference's loc_qpts, src/operators.cpp:305-316)
+// for integrateError: node shape functions there [nQ][nN], the solution-point
+// interpolation opp_spts_to_qpts [nQ][nS] and the weights [nQ] in
+// getQptWeights's order (src/points.cpp:347-374).
+bool quad_tables(int nDims, int P, int nNodes, int quadOrder, std::vector<double> &shapeQ,
+                 std::vector<double> &interpQ, std::vector<double> &wq, std::string &err);
+// Node shape functions at the solution points [nS][nN].
+bool spt_shape_table(int nDims, int P, int nNodes, std::vector<double> &shapeS, std::string &err);
 // Lagrange interpolation between the solution points of two orders
 // ([nS_to][nS_from], the restart's inter-order operator, src/ele.cpp:1506-1555).
 void order_interp(int nDims, int Pfrom, int Pto, std::vector<double> &out);

@@ -6,6 +6,7 @@
 #include "dispatch.h"
 #include "kernels.cuh"
 #include "kernels_tma.cuh"
+#include "kernels_visc_tma.cuh"
 #include "optab_upload.cuh"
 
 namespace frg {
@@ -143,6 +144,45 @@ bool make_set(KernelSet &k, std::string &err) {
   return true;
 }
 
+// 3D viscous TMA passes: tiles of 4 (FP32) or 2 (FP64) elements, the 16-byte
+// minimum row of a TMA box; 128 threads for the gradient pass (three blocks
+// per SM), 256 for the stage pass (two blocks per SM, by shared memory)
+template <typename S>
+constexpr int visc_tma_te() { return sizeof(S) == 4 ? 4 : 2; }
+constexpr int kViscGradNT = 128, kViscStageNT = 256;
+template <class C, typename R, typename S, bool BC>
+void launch_visc3_grad(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
+  fr_visc3_grad_tma_kernel<C, R, S, BC, visc_tma_te<S>(), kViscGradNT><<<nBlk, kViscGradNT, smem, st>>>(
+      *static_cast<const StageArgs *>(args), *static_cast<const ViscMaps *>(maps));
+}
+template <class C, typename R, typename S, bool BC, int RS>
+void launch_visc3_stage(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
+  fr_visc3_stage_tma_kernel<C, R, S, BC, RS, visc_tma_te<S>(), kViscStageNT><<<nBlk, kViscStageNT, smem, st>>>(
+      *static_cast<const StageArgs *>(args), *static_cast<const ViscMaps *>(maps));
+}
+template <class C, typename R, typename S, bool BC, int RS>
+cudaError_t add_visc3_tma(KernelSet &k) {
+  constexpr int TE = visc_tma_te<S>();
+  using TG = VGradT<C, R, S, TE, kViscGradNT>;
+  using TS = VStageT<C, R, S, TE, kViscStageNT>;
+  if (TG::SMEM > 227 * 1024 || TS::SMEM > 227 * 1024) return cudaSuccess;  // not offered
+  auto fg = fr_visc3_grad_tma_kernel<C, R, S, BC, TE, kViscGradNT>;
+  auto fs = fr_visc3_stage_tma_kernel<C, R, S, BC, RS, TE, kViscStageNT>;
+  cudaError_t e = cudaFuncSetAttribute(fg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(fs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fg, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fs, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  k.vgrad = &launch_visc3_grad<C, R, S, BC>;
+  k.vstage = &launch_visc3_stage<C, R, S, BC, RS>;
+  k.vTE = TE;
+  k.vgradSmem = TG::SMEM;
+  k.vstageSmem = TS::SMEM;
+  return cudaSuccess;
+}
+
 template <class C, typename R, typename S, bool BC, int RS>
 bool make_set_visc(KernelSet &k, std::string &err) {
   using T = TileV<C, R>;
@@ -165,6 +205,8 @@ bool make_set_visc(KernelSet &k, std::string &err) {
     cudaFuncAttributes fa;  // load the trace kernel now (see make_set)
     e = cudaFuncGetAttributes(&fa, fr_trace_kernel<C, R, S>);
   }
+  if constexpr (C::DIM == 3)
+    if (e == cudaSuccess) e = add_visc3_tma<C, R, S, BC, RS>(k);
   if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
   return true;
 }

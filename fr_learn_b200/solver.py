@@ -117,6 +117,10 @@ def lib():
         "frg_residual_vjp": ([vp, vp, vp, vp, C.POINTER(d)], i),
         "frg_adjoint_forward": ([vp, i, i], i),
         "frg_adjoint_backward": ([vp, vp, vp, vp, C.POINTER(d)], i),
+        "frg_read_gmsh": ([C.c_char_p, C.c_char_p, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp, vp, vp], i),
+        "frg_wall_force": ([vp, vp], i),
+        "frg_mass_flux": ([vp, i, vp], i),
+        "frg_integrate_error": ([vp, i, d, i, i, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -279,6 +283,24 @@ class Solver:
         _check(lib().frg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(it)))
         return it.value
 
+    # -- output integrals (solver::computeWallForce / computeMassFlux /
+    #    integrateError) of the current solution
+    def computeWallForce(self):
+        out = np.zeros(6)
+        _check(lib().frg_wall_force(self.h, out.ctypes.data))
+        return out
+
+    def computeMassFlux(self, errorNorm=0):
+        out = np.zeros(self.nFields)
+        _check(lib().frg_mass_flux(self.h, errorNorm, out.ctypes.data))
+        return out
+
+    def integrateError(self, icType, errorNorm=1, quadOrder=10, box=(-5.0, 5.0, -5.0, 5.0), eps=5.0):
+        out = np.zeros(self.nFields)
+        b = np.ascontiguousarray(box, np.float64)
+        _check(lib().frg_integrate_error(self.h, icType, eps, errorNorm, quadOrder, b.ctypes.data, out.ctypes.data))
+        return out
+
     def sync(self):
         _check(lib().frg_sync(self.h))
 
@@ -431,6 +453,25 @@ def read_restart_host(nEles, dataFileName, restartIter, **params):
     _check(lib().frg_read_restart_host(C.byref(p), int(nEles), os.fsencode(dataFileName), int(restartIter),
                                        U.ctypes.data, C.byref(t)))
     return U, t.value
+
+
+def read_gmsh(fileName, meshBounds) -> Mesh:
+    """geo::readGmsh: a Gmsh v2 ASCII file as a Mesh.  meshBounds maps the
+    file's physical names to boundary conditions like the reference's
+    ``mesh_bound`` lines: a dict {name: bc} or a "name bc; name bc" string,
+    with one name mapped to "fluid" (the volume)."""
+    if isinstance(meshBounds, dict):
+        meshBounds = "; ".join(f"{k} {v}" for k, v in meshBounds.items())
+    d, nE, nN = C.c_int(), C.c_int(), C.c_int()
+    fn, mb = os.fsencode(fileName), meshBounds.encode()
+    _check(lib().frg_read_gmsh(fn, mb, C.byref(d), C.byref(nE), C.byref(nN), None, None, None))
+    nd, ne, nn = d.value, nE.value, nN.value
+    xv = np.empty((ne, nn, nd), np.float64)
+    c2v = np.empty((ne, 4 if nd == 2 else 8), np.int32)
+    bc = np.empty((ne, 4 if nd == 2 else 6), np.int32)
+    _check(lib().frg_read_gmsh(fn, mb, C.byref(d), C.byref(nE), C.byref(nN), xv.ctypes.data, c2v.ctypes.data,
+                               bc.ctypes.data))
+    return Mesh(nd, xv, c2v, bc)
 
 
 class Ensemble:

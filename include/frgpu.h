@@ -159,6 +159,20 @@ frg_status frg_write_paraview_host(const frg_params *params, const frg_mesh *mes
 frg_status frg_read_restart_host(const frg_params *params, int nEles, const char *dataFileName, int restartIter,
                                  double *U, double *time);
 
+/* geo::readGmsh (src/geo.cpp:448-769) with the boundary matching of
+ * geo::processConn3D (src/geo.cpp:169-193): a Gmsh v2 ASCII file into the
+ * frg_mesh arrays.  meshBounds maps the file's physical names to boundary
+ * conditions as the reference's "mesh_bound <name> <bc>" input lines do:
+ * "<name> <bc>" pairs separated by ';' or newlines (case-insensitive), one of
+ * them "<volume name> fluid".  Volumes: 8-node hexahedra (Gmsh type 5) in 3D,
+ * 4-, 9- or 16-node quads (types 3, 10, 36) in 2D.  A face no other element
+ * shares takes the condition of the first boundary (in $PhysicalNames order)
+ * whose boundary elements hold all its corners.  With xv, c2v and bc all NULL
+ * only the sizes are returned; else xv [nEles][nNodes][nDims], c2v
+ * [nEles][4 or 8] (0-based vertex ids) and bc [nEles][4 or 6] are filled. */
+frg_status frg_read_gmsh(const char *fileName, const char *meshBounds, int *nDims, int *nEles, int *nNodes,
+                         double *xv, int *c2v, int *bc);
+
 frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, int *nEles);
 
 /* Dense operator matrices, row-major, as oper::setupOperators builds them:
@@ -333,6 +347,39 @@ frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery);
  * then reversed stage by stage.  The solution is left at U_N. */
 frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const double *thetaDir, double *lam0_host,
                                 double *thetaBar);
+
+/* ---- Output integrals of the current solution ---------------------------
+ * Evaluated on the device from the current state's traces (and, for viscous
+ * runs, its corrected gradient), i.e. on the face data a calcResidual(0) of
+ * the current state would leave. */
+
+/* solver::computeWallForce (src/solver.cpp:1367-1378) summing
+ * boundFace::computeWallForce (src/boundFace.cpp:330-378) over the slip,
+ * adiabatic and isothermal wall faces: force[0..2] the pressure force
+ * (sum of p n dA w), force[3..5] the viscous force (minus the stress tensor
+ * viscousStressTensor, src/flux.cpp:228-358, times n dA w); zeros for
+ * advection. */
+frg_status frg_wall_force(frg_solver *s, double *force /*[6]*/);
+/* solver::computeMassFlux (src/solver.cpp:1380-1391) summing
+ * boundFace::computeMassFlux (src/boundFace.cpp:380-418) over the
+ * characteristic, supersonic and subsonic in- and outflow faces: the
+ * faces' common normal flux Fn (Rusanov on the ghost state, plus the
+ * viscous part) times dA w (errorNorm 0), |Fn| dA w n_x (1) or
+ * (Fn dA)^2 w n_x (2). */
+frg_status frg_mass_flux(frg_solver *s, int errorNorm, double *flux /*[nFields]*/);
+/* solver::integrateError (src/solver.cpp:1507-1574) with calcError
+ * (src/funcs.cpp:1875-1979) for testCase 1.  icType selects the analytic
+ * solution: Navier-Stokes 0 (entropy error of the freestream rhoBound /
+ * pBound) or 1 (isentropic vortex of strength eps, 5 in the reference);
+ * advection 0 (Gaussian), 1 (sine wave), 2 (cosine product).  box =
+ * {xmin, xmax, ymin, ymax}, the period of the convected solution (the
+ * reference's mesh box, or +-5 for a mesh it reads).  errorNorm 0: the
+ * integral of state minus solution and of the state at the solution points,
+ * returned as |difference|; 1 / 2: the state and detJ interpolated to the
+ * Gauss points of quadOrder and |error| / error^2 integrated (2: the square
+ * root of the sum). */
+frg_status frg_integrate_error(frg_solver *s, int icType, double eps, int errorNorm, int quadOrder,
+                               const double *box, double *err /*[nFields]*/);
 
 /* Device-side launch counter: kernels launched by this handle so far. */
 frg_status frg_launch_count(const frg_solver *s, long long *count);

@@ -1402,4 +1402,248 @@ void orc_residual_norm(const orc_solver *s, int normType, double *out) {
   }
 }
 
+/* Gauss-Legendre nodes and weights of n points, ascending, by Newton's
+ * method on the Legendre polynomial (the reference tabulates them to 16
+ * digits, src/points.cpp:169-248, :376-470; the values agree to rounding). */
+static void gaussLegendre(int n, vector<double> &x, vector<double> &w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    double z = -cos(PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; k++) {
+        double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      if (n == 1) { p1 = z; p0 = 1.0; }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      double dz = p1 / dp;
+      z -= dz;
+      if (std::abs(dz) < 1e-16) break;
+    }
+    double p0 = 1.0, p1 = z;
+    for (int k = 2; k <= n; k++) {
+      double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    if (n == 1) { p1 = z; p0 = 1.0; }
+    dp = n * (z * p1 - p0) / (z * z - 1.0);
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+/* viscousStressTensor (src/flux.cpp:228-358) */
+static void stressTensor(const orc_params &p, int d, const double *U, const double *g /*[d][nV]*/, double tau[3][3]) {
+  int nV = d + 2;
+  auto G = [&](int a, int b) { return g[a * nV + b]; };
+  double rho = U[0], u = U[1] / rho, v = U[2] / rho;
+  double e = U[d + 1] / rho - 0.5 * (u * u + v * v), w = 0.;
+  if (d == 3) { w = U[3] / rho; e -= 0.5 * (w * w); }
+  double dRho_dx = G(0, 0), dRhoU_dx = G(0, 1), dRhoV_dx = G(0, 2);
+  double dRho_dy = G(1, 0), dRhoU_dy = G(1, 1), dRhoV_dy = G(1, 2);
+  double dRho_dz = 0, dRhoU_dz = 0, dRhoW_dz = 0;
+  if (d == 3) { dRho_dz = G(2, 0); dRhoU_dz = G(2, 1); dRhoW_dz = G(2, 3); }
+  double mu = p.mu_inf;
+  if (!p.fixVis) {
+    double rt = (p.gamma - 1.0) * e / p.rt_inf;
+    mu *= pow(rt, 1.5) * (1. + p.c_sth) / (rt + p.c_sth);
+  }
+  double du_dx = (dRhoU_dx - dRho_dx * u) / rho, du_dy = (dRhoU_dy - dRho_dy * u) / rho;
+  double dv_dx = (dRhoV_dx - dRho_dx * v) / rho, dv_dy = (dRhoV_dy - dRho_dy * v) / rho;
+  double du_dz = 0, dw_dz = 0;
+  if (d == 3) { du_dz = (dRhoU_dz - dRho_dz * u) / rho; dw_dz = (dRhoW_dz - dRho_dz * w) / rho; }
+  double diag = (du_dx + dv_dy + dw_dz) / 3.0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) tau[i][j] = 0;
+  tau[0][0] = 2.0 * mu * (du_dx - diag);
+  tau[1][1] = 2.0 * mu * (dv_dy - diag);
+  tau[0][1] = tau[1][0] = mu * (du_dy + dv_dx);
+  if (d == 3) {
+    tau[0][2] = tau[2][0] = mu * (du_dz + dv_dx);
+    tau[1][2] = tau[2][1] = mu * (du_dz + dv_dy);
+    tau[2][2] = 2.0 * mu * (dw_dz - diag);
+  }
+}
+
+/* solver::computeWallForce (src/solver.cpp:1367-1378) summing
+ * boundFace::computeWallForce (src/boundFace.cpp:330-378) over the slip,
+ * adiabatic and isothermal wall faces, from the face data of the last
+ * orc_calc_residual: force[0..2] pressure, force[3..5] viscous stress. */
+void orc_wall_force(const orc_solver *s, double *force) {
+  const orc_params &p = s->p;
+  int d = s->nDims, nV = s->nV, nE = s->nE, nF = s->nF, P = s->P;
+  vector<double> w = qptWeights1D(P);
+  for (int j = 0; j < 6; j++) force[j] = 0;
+  for (const OFace &F : s->faces) {
+    if (F.eR >= 0 || !(F.bc == BC_SLIP || F.bc == BC_ADI_NOSLIP || F.bc == BC_ISO_NOSLIP)) continue;
+    double ff[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < s->nFptFace; i++) {
+      double weight = d == 2 ? w[i] : w[i % (P + 1)] * w[i / (P + 1)];
+      int fl = F.fptL[i];
+      const double *U = &s->U_fpts[((size_t)fl * nE + F.eL) * nV];
+      const double *n = &s->norm_fpts[((size_t)fl * nE + F.eL) * d];
+      double dA = s->dA_fpts[(size_t)fl * nE + F.eL];
+      double rho = U[0], vMagSq = 0;
+      for (int dim = 0; dim < d; dim++) vMagSq += U[dim + 1] * U[dim + 1] / (rho * rho);
+      double pr = (p.gamma - 1) * (U[d + 1] - 0.5 * rho * vMagSq);
+      for (int dim = 0; dim < d; dim++) ff[dim] += pr * n[dim] * dA * weight;
+      if (p.viscous) {
+        double g[3 * 5], tau[3][3];
+        for (int dim = 0; dim < d; dim++)
+          for (int k = 0; k < nV; k++) g[dim * nV + k] = s->dU_fpts[s->i4(dim, fl, nF, F.eL, k)];
+        stressTensor(p, d, U, g, tau);
+        for (int a = 0; a < d; a++)
+          for (int b = 0; b < d; b++) ff[3 + a] -= tau[a][b] * n[b] * dA * weight;
+      }
+    }
+    for (int j = 0; j < 6; j++) force[j] += ff[j];
+  }
+}
+
+/* solver::computeMassFlux (src/solver.cpp:1380-1391) summing
+ * boundFace::computeMassFlux (src/boundFace.cpp:380-418) over the
+ * characteristic / supersonic / subsonic in- and outflow faces, from the
+ * faces' common fluxes of the last orc_calc_residual. */
+void orc_mass_flux(const orc_solver *s, int errorNorm, double *flux) {
+  int d = s->nDims, nV = s->nV, nE = s->nE, P = s->P;
+  vector<double> w = qptWeights1D(P);
+  for (int k = 0; k < nV; k++) flux[k] = 0;
+  for (const OFace &F : s->faces) {
+    if (F.eR >= 0 || !(F.bc == BC_CHAR || F.bc == BC_SUP_IN || F.bc == BC_SUP_OUT || F.bc == BC_SUB_IN ||
+                       F.bc == BC_SUB_OUT))
+      continue;
+    vector<double> ff(nV, 0.0);
+    for (int i = 0; i < s->nFptFace; i++) {
+      double weight = d == 2 ? w[i] : w[i % (P + 1)] * w[i / (P + 1)];
+      int fl = F.fptL[i];
+      double dA = s->dA_fpts[(size_t)fl * nE + F.eL];
+      double nx = s->norm_fpts[((size_t)fl * nE + F.eL) * d];
+      const double *Fn = &F.Fn[(size_t)i * nV];
+      for (int k = 0; k < nV; k++) {
+        if (errorNorm == 0) ff[k] += Fn[k] * dA * weight;
+        else if (errorNorm == 1) ff[k] += std::abs(Fn[k]) * dA * weight * nx;
+        else ff[k] += (Fn[k] * dA) * (Fn[k] * dA) * weight * nx;
+      }
+    }
+    for (int k = 0; k < nV; k++) flux[k] += ff[k];
+  }
+}
+
+/* calcError (src/funcs.cpp:1875-1979), testCase 1: the state minus the
+ * analytic solution at x (icType 0 entropy error / Gaussian, 1 isentropic
+ * vortex of strength eps / sine wave, 2 cosine product for advection);
+ * box = xmin, xmax, ymin, ymax of the periodic domain. */
+static void calcError(const orc_params &p, int d, int icType, double eps, const double *box, double time,
+                      const double *U, const double *x, int errorNorm, double *err) {
+  int nV = p.equation == 0 ? 1 : d + 2;
+  double xmin = box[0], xmax = box[1], ymin = box[2], ymax = box[3];
+  for (int k = 0; k < nV; k++) err[k] = 0;
+  if (p.equation == 1) {
+    double gamma = p.gamma;
+    if (icType == 0) {
+      double pfs = p.pBound, rhofsg = pow(p.rhoBound, gamma);
+      double rho = U[0], u = U[1] / rho, v = U[2] / rho, w = d == 2 ? 0 : U[3] / rho;
+      double pr = (gamma - 1.) * (U[d + 1] - .5 * rho * (u * u + v * v + w * w));
+      err[0] = pr * rhofsg / (pow(rho, gamma) * pfs) - 1.;
+    } else {
+      double X = fmod((x[0] - time), (xmax - xmin)), Y = fmod((x[1] - time), (ymax - ymin));
+      if (X > xmax) X -= (xmax - xmin);
+      if (Y > ymax) Y -= (ymax - ymin);
+      if (X < xmin) X += (xmax - xmin);
+      if (Y < ymin) Y += (ymax - ymin);
+      double f = 1.0 - (X * X + Y * Y);
+      double rho = max(pow(1. - eps * eps * (gamma - 1.) / (8. * gamma * PI * PI) * exp(f), 1.0 / (gamma - 1.0)), 1e-10);
+      double vx = 1. - eps * Y / (2. * PI) * exp(f / 2.), vy = 1. + eps * X / (2. * PI) * exp(f / 2.);
+      double pr = pow(rho, gamma);
+      err[0] = rho;
+      err[1] = rho * vx;
+      err[2] = rho * vy;
+      if (d == 3) err[3] = 0.;
+      err[d + 1] = pr / (gamma - 1) + (0.5 * rho * (vx * vx + vy * vy));
+      for (int k = 0; k < nV; k++) err[k] = U[k] - err[k];
+    }
+  } else {
+    double X = std::abs(fmod((x[0] - time), (xmax - xmin))), Y = std::abs(fmod((x[1] - time), (ymax - ymin)));
+    if (X > (xmax - xmin) / 2) X -= (xmax - xmin);
+    if (Y > (ymax - ymin) / 2) Y -= (ymax - ymin);
+    if (icType == 0) err[0] = exp(-(X * X + Y * Y));
+    else if (icType == 1) err[0] = 1 + sin(2. * PI * (x[0] + 5. - time) / 10.);
+    else err[0] = cos(2 * PI * x[0] / 6.) * cos(2 * PI * x[1] / 6.) * cos(2 * PI * (d == 3 ? x[2] : 0.0) / 6.);
+    err[0] = U[0] - err[0];
+  }
+  if (errorNorm == 1)
+    for (int k = 0; k < nV; k++) err[k] = std::abs(err[k]);
+  else if (errorNorm == 2)
+    for (int k = 0; k < nV; k++) err[k] *= err[k];
+}
+
+/* solver::integrateError (src/solver.cpp:1507-1574), testCase 1: errorNorm
+ * 0 integrates state minus solution and the state at the solution points and
+ * returns |difference|; 1 / 2 interpolate the state and detJ to the
+ * Gauss points of quadOrder (oper::setupInterpolateSptsQpts,
+ * src/operators.cpp:305-316) and integrate |error| / error^2 (2: square
+ * root of the sum).  eps is the vortex strength (5 for icType 1). */
+void orc_integrate_error(const orc_solver *s, int icType, double eps, int errorNorm, int quadOrder,
+                         const double *box, double *out) {
+  const orc_params &p = s->p;
+  int d = s->nDims, nV = s->nV, nE = s->nE, nS = s->nS, nN = s->nNodes, P = s->P;
+  for (int k = 0; k < nV; k++) out[k] = 0;
+  vector<double> err(nV);
+  if (errorNorm == 0) {
+    vector<double> wts = qptWeights(P, d), intU(nV, 0.0);
+    for (int e = 0; e < nE; e++)
+      for (int sp = 0; sp < nS; sp++) {
+        const double *U = &s->U[((size_t)sp * nE + e) * nV];
+        calcError(p, d, icType, eps, box, s->time, U, &s->pos_spts[((size_t)sp * nE + e) * d], 0, err.data());
+        double wd = s->detJ_spts[(size_t)sp * nE + e];
+        for (int k = 0; k < nV; k++) {
+          out[k] += err[k] * wts[sp] * wd;
+          intU[k] += U[k] * wts[sp] * wd;
+        }
+      }
+    for (int k = 0; k < nV; k++) out[k] = std::abs(out[k] - intU[k]);
+    return;
+  }
+  int nq1 = quadOrder + 1, nQ = d == 2 ? nq1 * nq1 : nq1 * nq1 * nq1;
+  vector<double> xq, wq1;
+  gaussLegendre(nq1, xq, wq1);
+  vector<double> wq(nQ);
+  vector<double> loc((size_t)nQ * 3, 0.0);
+  for (int q = 0; q < nQ; q++) {
+    int a = q % nq1, b = (q / nq1) % nq1, c = q / (nq1 * nq1);
+    loc[3 * q] = xq[a];
+    loc[3 * q + 1] = xq[b];
+    if (d == 3) loc[3 * q + 2] = xq[c];
+    wq[q] = d == 2 ? wq1[b] * wq1[a] : wq1[c] * wq1[b] * wq1[a]; /* getQptWeights ordering */
+  }
+  /* opp_spts_to_qpts (setupInterpolateSptsIpts, src/operators.cpp:259-302) */
+  vector<double> sp = gaussPts(P), A((size_t)nQ * nS);
+  for (int q = 0; q < nQ; q++)
+    for (int t = 0; t < nS; t++) {
+      int i = t % (P + 1), j = (t / (P + 1)) % (P + 1), k = t / ((P + 1) * (P + 1));
+      double v = Lagrange(sp, loc[3 * q], i) * Lagrange(sp, loc[3 * q + 1], j);
+      if (d == 3) v *= Lagrange(sp, loc[3 * q + 2], k);
+      A[(size_t)q * nS + t] = v;
+    }
+  vector<double> Uq((size_t)nQ * nE * nV), dq((size_t)nQ * nE), sh(nN), tmp(nN * 3);
+  dgemm(nQ, nE * nV, nS, 1.0, A.data(), s->U.data(), 0.0, Uq.data());
+  dgemm(nQ, nE, nS, 1.0, A.data(), s->detJ_spts.data(), 0.0, dq.data());
+  for (int e = 0; e < nE; e++)
+    for (int q = 0; q < nQ; q++) {
+      if (d == 2) shapeQuad(loc[3 * q], loc[3 * q + 1], nN, sh.data(), nullptr);
+      else shapeHex8(loc[3 * q], loc[3 * q + 1], loc[3 * q + 2], sh.data(), nullptr);
+      double x[3] = {0, 0, 0};
+      for (int n = 0; n < nN; n++)
+        for (int dim = 0; dim < d; dim++) x[dim] += sh[n] * s->nodes[((size_t)n * nE + e) * d + dim];
+      calcError(p, d, icType, eps, box, s->time, &Uq[((size_t)q * nE + e) * nV], x, errorNorm, err.data());
+      for (int k = 0; k < nV; k++) out[k] += err[k] * wq[q] * dq[(size_t)q * nE + e];
+    }
+  if (errorNorm == 2)
+    for (int k = 0; k < nV; k++) out[k] = std::sqrt(std::abs(out[k]));
+}
+
 }  // extern "C"

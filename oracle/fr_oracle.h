@@ -88,6 +88,13 @@ int orc_get_iter(const orc_solver *s);
 /* ele::getNormResidual summed as writeResidual does (src/output.cpp:846) */
 void orc_residual_norm(const orc_solver *s, int normType, double *out);
 void orc_set_threads(int n);
+/* Integrals of the output path (computeWallForce, computeMassFlux,
+ * integrateError); the first two use the face data of the last
+ * orc_calc_residual. */
+void orc_wall_force(const orc_solver *s, double *force /*[6]*/);
+void orc_mass_flux(const orc_solver *s, int errorNorm, double *flux /*[nFields]*/);
+void orc_integrate_error(const orc_solver *s, int icType, double eps, int errorNorm, int quadOrder,
+                         const double *box /*xmin, xmax, ymin, ymax*/, double *out /*[nFields]*/);
 
 /* Pointwise routines, exposed for known-answer tests against the reference.
  * Fluxes are [nDims][nFields]; gradU is [nDims][nFields]. */

@@ -433,6 +433,50 @@ static int modeVtu(char *inputFile, const char *out, int nsteps) {
   return 0;
 }
 
+/* The output integrals after nsteps updates and one calcResidual(0):
+ * solver::computeWallForce, computeMassFlux (errorNorm 0, 1, 2) and, with
+ * testCase 1, integrateError (errorNorm 0, 1, 2; quadOrder from the input). */
+static int modeIntegrals(char *inputFile, const char *out, int nsteps) {
+  openOut(out);
+  input params;
+  params.rank = 0;
+  params.nproc = 1;
+  params.readInputFile(inputFile);
+  solver S;
+  S.setup(&params, params.order);
+  S.initializeSolution();
+  double prm[] = {params.gamma, params.rhoBound, params.uBound, params.vBound, params.wBound,
+                  params.pBound, params.mu_inf, params.prandtl, params.c_sth, params.rt_inf,
+                  (double)params.fixVis, params.penFact, params.tau, params.TWall, params.RGas,
+                  params.uWall, params.vWall, params.wWall, params.dt, params.CFL};
+  dump("params", prm, sizeof(prm) / sizeof(double), {(int)(sizeof(prm) / sizeof(double))});
+  params.iter = params.initIter;
+  for (int n = 0; n < nsteps; n++) {
+    params.iter++;
+    S.update();
+  }
+  const int nS = S.nSpts, nE = S.nEles;
+  dumpArr("U_spts", S.U_spts, {nS, nE, (int)params.nFields});
+  double t = params.time;
+  dump("time", &t, 1, {1});
+  S.calcResidual(0);
+  std::vector<double> f = S.computeWallForce();
+  dump("wall_force", f.data(), f.size(), {(int)f.size()});
+  for (int en = 0; en < 3; en++) {
+    params.errorNorm = en;
+    std::vector<double> m = S.computeMassFlux();
+    dump("mass_flux_" + std::to_string(en), m.data(), m.size(), {(int)m.size()});
+  }
+  params.testCase = 1;
+  for (int en = 0; en < 3; en++) {
+    params.errorNorm = en;
+    std::vector<double> e = S.integrateError();
+    dump("error_" + std::to_string(en), e.data(), e.size(), {(int)e.size()});
+  }
+  fclose(g_manifest);
+  return 0;
+}
+
 static int modeTime(char *inputFile, int nsteps) {
   input params;
   params.rank = 0;
@@ -473,6 +517,7 @@ int main(int argc, char **argv) {
   if (mode == "case" && argc == 5) return modeCase(argv[2], argv[3], atoi(argv[4]));
   if (mode == "time" && argc == 4) return modeTime(argv[2], atoi(argv[3]));
   if (mode == "vtu" && argc == 5) return modeVtu(argv[2], argv[3], atoi(argv[4]));
+  if (mode == "integrals" && argc == 5) return modeIntegrals(argv[2], argv[3], atoi(argv[4]));
   fprintf(stderr, "bad arguments\n");
   return 2;
 }

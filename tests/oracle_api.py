@@ -64,6 +64,10 @@ def lib():
         L.orc_time_step_b.argtypes = [C.c_void_p, C.c_int]
         L.orc_residual_norm.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_wall_force.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_mass_flux.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_integrate_error.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                          C.c_void_p]
         _lib = L
     return _lib
 
@@ -162,4 +166,20 @@ class Oracle:
     def residual_norm(self, norm_type=2):
         out = np.zeros(self.nV)
         lib().orc_residual_norm(self.h, norm_type, out.ctypes.data)
+        return out
+
+    def wall_force(self):
+        out = np.zeros(6)
+        lib().orc_wall_force(self.h, out.ctypes.data)
+        return out
+
+    def mass_flux(self, error_norm=0):
+        out = np.zeros(self.nV)
+        lib().orc_mass_flux(self.h, error_norm, out.ctypes.data)
+        return out
+
+    def integrate_error(self, ic_type, error_norm=1, quad_order=10, box=(-5.0, 5.0, -5.0, 5.0), eps=5.0):
+        out = np.zeros(self.nV)
+        b = np.ascontiguousarray(box, np.float64)
+        lib().orc_integrate_error(self.h, ic_type, eps, error_norm, quad_order, b.ctypes.data, out.ctypes.data)
         return out

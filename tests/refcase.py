@@ -134,3 +134,18 @@ def run_kat():
     out = tempfile.mkdtemp(prefix="frkat_")
     subprocess.run([HARNESS, "kat", out], check=True, stdout=subprocess.DEVNULL)
     return load(out)
+
+
+def run_integrals(mesh, nsteps=0, workdir=None, **kw):
+    """Run the harness 'integrals' mode: the state after nsteps updates and
+    the reference's computeWallForce / computeMassFlux / integrateError."""
+    if not os.path.exists(HARNESS):
+        build()
+    wd = workdir or tempfile.mkdtemp(prefix="frref_")
+    msh = os.path.join(wd, "mesh.msh")
+    bcnames = write_gmsh(mesh, msh)
+    inp = os.path.join(wd, "input.txt")
+    write_input(inp, msh, bcnames, **kw)
+    out = os.path.join(wd, "out")
+    subprocess.run([HARNESS, "integrals", inp, out, str(nsteps)], check=True, cwd=wd, stdout=subprocess.DEVNULL)
+    return load(out)

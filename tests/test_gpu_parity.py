@@ -295,3 +295,51 @@ def test_advection_config1_full_run(oracle):
     o.update(1000)
     assert relerr(g.get("U_spts"), o.U()) < FP64_TOL
     assert abs(g.time - o.time) <= 1e-12 * o.time
+
+
+def _visc3_cases():
+    from fr_learn_b200 import box3d
+
+    return {
+        "tgv_periodic": (box3d(4, 3, 5, (0, 0, 0), (2 * np.pi,) * 3, perturb=0.05, seed=41), 10, 0.1,
+                         dict(order=3, viscous=1, mu_inf=1.0 / 1600, prandtl=0.71, fixVis=1, penFact=0.0, tau=1.0,
+                              dtType=0, dt=1e-3)),
+        "walls_penalty": (box3d(3, 3, 3, (-2, -2, -1), (2, 2, 1),
+                                bcs={"zmin": "adiabatic_noslip", "zmax": "isothermal_noslip"}, perturb=0.1,
+                                seed=42), 1, 0.0,
+                          dict(order=2, viscous=1, mu_inf=0.01, prandtl=0.72, fixVis=1, penFact=0.3, tau=1.0,
+                               TWall=1.0, RGas=1.0 / 1.4, dtType=1, CFL=0.3)),
+        "advdiff_char": (box3d(3, 4, 3, (-2, -2, -2), (2, 2, 2),
+                               bcs={s: "char" for s in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")},
+                               perturb=0.1, seed=43), 0, 0.0,
+                         dict(order=3, equation=0, viscous=1, diffD=0.05, penFact=0.2, tau=1.0, dtType=0,
+                              dt=1e-3)),
+        "sutherland_p4": (box3d(3, 3, 3, (0, 0, 0), (2 * np.pi,) * 3, perturb=0.05, seed=44), 10, 0.1,
+                          dict(order=4, viscous=1, mu_inf=0.02, prandtl=0.71, fixVis=0, c_sth=0.41, rt_inf=2.5,
+                               penFact=0.0, tau=1.0, dtType=1, CFL=0.3)),
+    }
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("case", list(_visc3_cases()))
+def test_visc3_tma_kernels_match_generic_kernels(monkeypatch, precision, case):
+    """The 3D viscous TMA passes of the fused update (the stage input landed
+    in the padded point layout, the gradient recomputed in the stage pass,
+    the boundary viscous flux formed in the gradient pass) agree with the
+    generic per-thread-load kernels: to FP64 rounding (the TMA stage
+    multiplies by a stored 1/detJ where the generic one divides), in mixed
+    mode to FP32 rounding level."""
+    from fr_learn_b200 import Solver
+
+    mesh, ic, a0, kw = _visc3_cases()[case]
+    monkeypatch.setenv("FRG_KERNEL", "generic")
+    a = Solver(mesh, precision=precision, **kw)
+    monkeypatch.delenv("FRG_KERNEL")
+    b = Solver(mesh, precision=precision, **kw)
+    for s in (a, b):
+        s.setInitialCondition(ic, a0)
+        s.update(5)
+    assert relerr(b.get("U_spts"), a.get("U_spts")) < (1e-13 if precision == 0 else 1e-6)
+    assert relerr(b.get("U_fpts"), a.get("U_fpts")) < (1e-13 if precision == 0 else 1e-6)
+    if kw.get("dtType") == 1:
+        assert relerr(b.dt, a.dt) < (1e-13 if precision == 0 else 1e-6)
