@@ -288,6 +288,7 @@ def run_gpu(args, rank, world, local_rank):
     res["adjoint"] = run_adjoint_bump(stream)
     res["ensemble"] = run_ensemble(stream)
     res["tgv"] = run_tgv(stream, flush)
+    res["tgv"]["kinetic_energy_vs_fp64_oracle"] = run_tgv_oracle(stream)
     res["c1"] = run_advection_c1(stream)
     res["scale"] = run_scale(stream, flush)
     res["opgemm"] = run_operator_gemm(stream, flush)
@@ -623,6 +624,64 @@ def run_tgv(stream, flush, steps=50, warmup=3, hist_steps=400, hist_every=25):
         "dissipation_rate_fp64": eps_d.tolist(),
         "dissipation_rate_max_rel_diff": float(np.max(np.abs(eps_m - eps_d)) / np.max(np.abs(eps_d))),
     }
+    return out
+
+
+def run_tgv_oracle(stream, full_steps=2, small_n=8, small_steps=200, every=25):
+    """Kinetic energy of the Taylor-Green workload against the FP64 oracle
+    (the CPU restatement of the reference, on all host cores): (a) the full
+    32^3 mesh for `full_steps` steps, (b) the same physics on a small_n^3
+    mesh for `small_steps` steps, sampled every `every` steps, with the
+    dissipation rate -dE_k/dt; both GPU paths (mixed, FP64) beside the
+    oracle.  Bounded so the whole run stays within a few minutes."""
+    import torch
+
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver, box3d
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api
+
+    oracle_api.lib().orc_set_threads(max(1, min(os.cpu_count() or 1, 64)))
+    out = {}
+    for label, mesh, nsteps, samp in (("full_32x32x32", tgv_mesh(), full_steps, 1),
+                                      (f"small_{small_n}x{small_n}x{small_n}",
+                                       box3d(small_n, small_n, small_n, (0.0, 0.0, 0.0), (2 * np.pi,) * 3),
+                                       small_steps, every)):
+        t0 = time.perf_counter()
+        o = oracle_api.Oracle(oracle_api.params(nDims=3, **tgv_params()), mesh)
+        o.set_ic(10, TGV_MA)
+        detJ = o.get("detJac_spts").reshape(-1, mesh.nEles)
+        ke = {"oracle_fp64": [kinetic_energy(o.U(), detJ, TGV_P)]}
+        tt = [0.0]
+        for _ in range(nsteps // samp):
+            o.update(samp)
+            ke["oracle_fp64"].append(kinetic_energy(o.U(), detJ, TGV_P))
+            tt.append(o.time)
+        o_s = time.perf_counter() - t0
+        o.close()
+        for name, prec in (("gpu_mixed", FRG_MIXED), ("gpu_fp64", FRG_FP64)):
+            s = Solver(mesh, precision=prec, **tgv_params())
+            s.set_stream(stream.cuda_stream)
+            s.setInitialCondition(10, TGV_MA)
+            ke[name] = [kinetic_energy(s.get("U_spts"), detJ, TGV_P)]
+            with torch.cuda.stream(stream):
+                for _ in range(nsteps // samp):
+                    s.update(samp)
+                    stream.synchronize()
+                    ke[name].append(kinetic_energy(s.get("U_spts"), detJ, TGV_P))
+            s.set_stream(None)
+            s.close()
+        t = np.array(tt)
+        ref = np.array(ke["oracle_fp64"])
+        eps_ref = -np.gradient(ref, t)
+        r = {"steps": nsteps, "every": samp, "t": tt, "kinetic_energy": ke, "oracle_seconds": o_s}
+        for name in ("gpu_mixed", "gpu_fp64"):
+            k = np.array(ke[name])
+            r[f"{name}_max_rel_diff"] = float(np.max(np.abs(k - ref) / ref))
+            if len(t) > 2:
+                r[f"{name}_dissipation_rate_max_rel_diff"] = float(np.max(np.abs(-np.gradient(k, t) - eps_ref))
+                                                                   / np.max(np.abs(eps_ref)))
+        out[label] = r
     return out
 
 

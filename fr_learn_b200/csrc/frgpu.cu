@@ -996,6 +996,55 @@ frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out
   return FRG_OK;
 }
 
+frg_status frg_set_operators(frg_solver *s, int order, const double *E, const double *D, const double *C,
+                             const double *Efn) {
+  if (!s || !E || !D || !C) return fail(FRG_ERR_ARG, "null argument");
+  if (order != s->p.order) return fail(FRG_ERR_ARG, "operators of order %d for a solver of order %d", order, s->p.order);
+  if (s->adj) return fail(FRG_ERR_ARG, "operators cannot change once the adjoint is set up");
+  const int d = s->p.nDims, nS = s->nS, nF = s->nF;
+  // the given matrices against one scheme's tensor-product operators
+  auto matches = [&](const Ops1D &o) {
+    std::vector<double> m;
+    auto same = [&](const double *given, int which, int dim) {
+      dense_operator(d, o, which, dim, m);
+      double mx = 0, diff = 0;
+      for (size_t i = 0; i < m.size(); i++) {
+        mx = std::max(mx, std::fabs(m[i]));
+        diff = std::max(diff, std::fabs(m[i] - given[i]));
+      }
+      return diff <= 1e-13 * std::max(mx, 1.0);
+    };
+    if (!same(E, 0, 0) || !same(C, 3, 0)) return false;
+    for (int k = 0; k < d; k++) {
+      if (!same(D + (size_t)k * nS * nS, 1, k)) return false;
+      if (Efn && !same(Efn + (size_t)k * nF * nS, 2, k)) return false;
+    }
+    return true;
+  };
+  int scheme = -1;
+  for (int v : {s->p.vcjhScheme, 0, 1, 2, 3}) {
+    if (v == 3 && order < 2) continue;
+    if (matches(build_ops1d(order, v))) {
+      scheme = v;
+      break;
+    }
+  }
+  if (scheme < 0)
+    return fail(FRG_ERR_ARG, "the matrices are not the FR operators of a VCJH scheme (DG, SD, HU, C+) at order %d "
+                             "on the reference's Gauss points", order);
+  if (scheme != s->p.vcjhScheme) {
+    frg_status st;
+    if ((st = frg_sync(s))) return st;
+    s->p.vcjhScheme = scheme;
+    s->ops = build_ops1d(order, scheme);
+    drop_graphs(s);  // the captured stages carry the scheme
+    for (auto &r : s->opImg)
+      for (float *&q : r)
+        if (q) { cudaFree(q); q = nullptr; }
+  }
+  return FRG_OK;
+}
+
 frg_status frg_apply_operator(frg_solver *s, int which, int dim, const float *X, float *Y, int ld, float beta) {
   if (!s || !X || !Y) return fail(FRG_ERR_ARG, "null argument");
   if (which < 0 || which > 4) return fail(FRG_ERR_ARG, "operator %d does not exist", which);

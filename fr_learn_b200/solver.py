@@ -119,6 +119,7 @@ def lib():
         "frg_adjoint_backward": ([vp, vp, vp, vp, C.POINTER(d)], i),
         "frg_read_gmsh": ([C.c_char_p, C.c_char_p, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp, vp, vp], i),
         "frg_wall_force": ([vp, vp], i),
+        "frg_set_operators": ([vp, i, vp, vp, vp, vp], i),
         "frg_mass_flux": ([vp, i, vp], i),
         "frg_integrate_error": ([vp, i, d, i, i, vp, vp], i),
     }
@@ -194,6 +195,14 @@ class Solver:
         out = np.empty(shape, np.float64)
         _check(lib().frg_get_operator(self.h, which, dim, out.ctypes.data))
         return out
+
+    def set_operators(self, order, E, D, C, Efn=None):
+        """oper::setupOperators's matrices for the device path (see
+        include/frgpu.h frg_set_operators): E [nF][nS], D [nDims][nS][nS],
+        C [nS][nF], Efn [nDims][nF][nS] or None."""
+        arrs = [np.ascontiguousarray(a, np.float64) if a is not None else None for a in (E, D, C, Efn)]
+        ptrs = [a.ctypes.data if a is not None else None for a in arrs]
+        _check(lib().frg_set_operators(self.h, order, *ptrs))
 
     def apply_operator(self, which, dim, X_ptr, Y_ptr, ld, beta=0.0):
         """Y = Op X + beta Y on FP32 device arrays [nFields][points][ld] (the

@@ -181,6 +181,20 @@ frg_status frg_info(const frg_solver *s, int *nSpts, int *nFpts, int *nFields, i
  * 4 opp_correctU[dim] [nS][nF]. */
 frg_status frg_get_operator(const frg_solver *s, int which, int dim, double *out);
 
+/* The reference's operator matrices for the device path:
+ * oper::setupOperators (src/operators.cpp:13-76) builds them per order; a
+ * shim passes them here after frg_create.  E = opp_spts_to_fpts [nF][nS],
+ * D = opp_grad_spts [nDims][nS][nS], C = opp_correction [nS][nF], Efn =
+ * opp_extrapolateFn [nDims][nF][nS] (may be NULL), row-major.  The device
+ * path applies these operators as tensor products of 1D tables (sum
+ * factorisation), so the call identifies the matrices: they must be the FR
+ * operators, within 1e-13 relative, of one VCJH correction scheme (DG, SD,
+ * HU, C+) at the solver's order on the reference's Gauss points; the solver
+ * then uses that scheme (a change takes effect from the next call).
+ * FRG_ERR_ARG when they are not, or when the order differs. */
+frg_status frg_set_operators(frg_solver *s, int order, const double *E, const double *D, const double *C,
+                             const double *Efn);
+
 /* The operator applications of the `oper` object -- applySptsFpts (which 0),
  * applyGradSpts (1, one dim), applyExtrapolateFn (2, one dim),
  * applyCorrectDivF (3), applyCorrectGradU's parent-space product (4, one
