@@ -31,7 +31,7 @@ CU_SOURCES = ["frgpu.cu", "integrals.cu", "stage_2d_f64.cu", "stage_2d_f32.cu", 
 # unaffected by these flags, so the FP64 units stay exact.
 UNIT_FLAGS = {u: ["-prec-div=false", "-prec-sqrt=false"] for u in ("stage_2d_f32.cu", "stage_3d_f32.cu")}
 CXX_SOURCES = ["setup.cpp", "restart.cpp", "gmsh.cpp"]
-HEADERS = ["kernels.cuh", "kernels_tma.cuh", "kernels_visc_tma.cuh", "adjoint.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
+HEADERS = ["kernels.cuh", "kernels_tma.cuh", "kernels_visc_tma.cuh", "adjoint.cuh", "adjoint_visc.cuh", "adjoint_impl.cuh", "dual.cuh", "optab_upload.cuh",
            "physics.cuh", "setup.h", "dispatch.h", "stage_impl.cuh"]
 
 

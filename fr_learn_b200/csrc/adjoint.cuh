@@ -34,6 +34,17 @@
 
 namespace frg {
 
+// Scratch of the viscous adjoint (adjoint_visc.cuh), FP64 [..][point][element].
+struct AdjViscBufs {
+  double *g;      // forward corrected gradient at the solution points [DIM][NV][NS][L]
+  double *fvn;    // each side's projected viscous flux [NV][NF][L] (interior flux points)
+  double *fvn2;   // 3D LDG penalty: the left side's projection [NV][NF][L]
+  double *ub;     // state adjoint at the solution points [NV][NS][L]
+  double *ufb;    // trace adjoint at the flux points [NV][NF][L]
+  double *dcb;    // adjoint of the LDG correction Dc = Uc - U_f [NV][NF][L]
+  int visc2;
+};
+
 struct AdjArgs {
   int nE, nEle;           // element stride (padded) and real element count
   const double *Y;        // stage state [NV][NS][nE]
@@ -56,6 +67,7 @@ struct AdjArgs {
   const int *grp;         // ensemble mode: group of each element, else null
   const double *dtGrp;    // ensemble mode: fixed dt per group (replaces dt)
   double *thetaBar;       // += fbar . dFn/dtheta over boundary flux points
+  AdjViscBufs v;          // viscous runs only
   Phys ph;
 };
 

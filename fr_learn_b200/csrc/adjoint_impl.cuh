@@ -2,6 +2,7 @@
 // kernels; included once per dimension unit after defining FRG_ADJ_DIM.
 #pragma once
 #include "adjoint.cuh"
+#include "adjoint_visc.cuh"
 #include "dispatch.h"
 #include "optab_upload.cuh"
 
@@ -33,6 +34,58 @@ void launch_wallp(const double *U, const int *nbr, const double *dA, const doubl
   fr_obj_wallp_kernel<C><<<(nE + 127) / 128, 128, 0, st>>>(U, nbr, dA, wsurf, vcjh, nE, L, bcWall, ph, grad, part);
 }
 
+// Viscous residuals: the forward gradient / projected-flux pass (the
+// generic gradient kernel on the stage state), then the two adjoint passes.
+template <class C, bool BC, int RS>
+void launch_adjv_elem(const AdjArgs &a, cudaStream_t st) {
+  using TV = TileV<C, double>;
+  StageArgs f{};
+  f.nE = a.nE;
+  f.nEle = a.nEle;
+  f.ldU = a.nE;
+  f.Uin_d = a.Y;
+  f.trIn = a.trY;
+  f.nbr = a.nbr;
+  f.nrm = a.nrm;
+  f.dA = a.dA;
+  f.JG = a.JG;
+  f.detJ = a.detJ;
+  f.err = a.err;
+  f.vcjh = a.vcjh;
+  f.flags = SF_RESIDUAL;
+  f.fvnOut = a.v.fvn;
+  f.fvn2Out = a.v.fvn2;
+  f.visc2 = a.v.visc2;
+  f.dUg = a.v.g;
+  f.ph = a.ph;
+  fr_visc_grad_kernel<C, double, double, BC><<<(a.nEle + TV::TE - 1) / TV::TE, C::NT, TV::SMEM, st>>>(f);
+  using T = AdjViscTile<C>;
+  fr_adjv_elem_kernel<C, BC, RS><<<(a.nEle + T::TE - 1) / T::TE, T::NT, T::SMEM, st>>>(a);
+  fr_adjv_out_kernel<C, BC><<<(a.nEle + 3) / 4, 128, 0, st>>>(a);
+}
+
+template <class C, bool BC, int RS>
+bool make_adjv(AdjSet &k, std::string &err) {
+  using T = AdjViscTile<C>;
+  using TV = TileV<C, double>;
+  k.face = &launch_adj_face<C>;
+  k.elem = &launch_adjv_elem<C, BC, RS>;
+  k.TE = T::TE;
+  k.elemLaunches = 3;
+  if constexpr (C::NV > 1) {
+    k.entropy = &launch_entropy<C>;
+    k.wallp = &launch_wallp<C>;
+    k.entropyBlocks = kAdjGrid;
+  }
+  cudaError_t e = cudaFuncSetAttribute(fr_adjv_elem_kernel<C, BC, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)T::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fr_visc_grad_kernel<C, double, double, BC>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV::SMEM);
+  if (e != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
+  return true;
+}
+
 template <class C, bool BC, int RS>
 bool make_adj(AdjSet &k, std::string &err) {
   using T = AdjTile<C>;
@@ -50,14 +103,21 @@ bool make_adj(AdjSet &k, std::string &err) {
   return true;
 }
 
+template <class C, bool BC, int RS>
+bool make_adj(AdjSet &k, std::string &err, bool viscous) {
+  if (viscous) return make_adjv<C, BC, RS>(k, err);
+  return make_adj<C, BC, RS>(k, err);
+}
+
 template <int DIM, int P, int NV>
 bool adj_variant(const KernelKey &key, AdjSet &k, std::string &err) {
   using C = Cfg<DIM, P, NV>;
+  const bool v = key.viscous != 0;
   if constexpr (NV == 1 || DIM == 3) {
-    return key.bc ? make_adj<C, true, 0>(k, err) : make_adj<C, false, 0>(k, err);
+    return key.bc ? make_adj<C, true, 0>(k, err, v) : make_adj<C, false, 0>(k, err, v);
   } else {
-    if (key.riemann == 1) return key.bc ? make_adj<C, true, 1>(k, err) : make_adj<C, false, 1>(k, err);
-    return key.bc ? make_adj<C, true, 0>(k, err) : make_adj<C, false, 0>(k, err);
+    if (key.riemann == 1) return key.bc ? make_adj<C, true, 1>(k, err, v) : make_adj<C, false, 1>(k, err, v);
+    return key.bc ? make_adj<C, true, 0>(k, err, v) : make_adj<C, false, 0>(k, err, v);
   }
 }
 
@@ -82,7 +142,6 @@ bool adj_order(const KernelKey &key, AdjSet &k, std::string &err) {
 #define FRG_ADJ_CAT(a, b) FRG_ADJ_CAT2(a, b)
 
 bool FRG_ADJ_CAT(select_adj_, FRG_ADJ_NAME)(const KernelKey &key, AdjSet &k, std::string &err) {
-  if (key.viscous) { err = "adjoint: viscous flux not supported"; return false; }
   if (key.precision != 0) { err = "adjoint: FP64 precision only"; return false; }
   if (key.NV == 1) return adj_order<FRG_ADJ_DIM, 1>(key, k, err);
   if (key.NV == FRG_ADJ_DIM + 2) return adj_order<FRG_ADJ_DIM, FRG_ADJ_DIM + 2>(key, k, err);

@@ -46,6 +46,7 @@ struct KernelSet {
   void (*vgrad)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
   void (*vstage)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
   int vTE = 0;
+  int vPadG = 0;  // points per padding slot of their tiles' point layout
   size_t vgradSmem = 0, vstageSmem = 0;
 };
 
@@ -65,6 +66,7 @@ struct AdjSet {
                 int bcWall, const Phys &ph, double *grad, double *part, cudaStream_t st) = nullptr;
   int entropyBlocks = 0;  // partial sums written by `entropy` (grid size)
   int TE = 0;             // elements per block of `elem`
+  int elemLaunches = 1;   // kernels `elem` launches (three for viscous residuals)
 };
 bool select_adj_2d(const KernelKey &key, AdjSet &k, std::string &err);
 bool select_adj_3d(const KernelKey &key, AdjSet &k, std::string &err);

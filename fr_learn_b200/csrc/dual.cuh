@@ -99,5 +99,11 @@ __device__ __forceinline__ Dual<N> pow(const Dual<N> &a, double e) {
   return r;
 }
 
+// x^e with a constant exponent given as a dual (its tangents are ignored)
+template <int N>
+__device__ __forceinline__ Dual<N> pow(const Dual<N> &a, const Dual<N> &e) {
+  return pow(a, e.v);
+}
+
 }  // namespace ad
 }  // namespace frg

@@ -497,12 +497,14 @@ frg_status setup_visc_tma(frg_solver *s) {
     const cuuint32_t box[2] = {te, (cuuint32_t)rows};
     return make_map_nd(m, base, dt, esz, 2, dims, str, box);
   };
-  // stage input in the padded point layout: the xi line walked with a box one
-  // point wider than the line (the extra point is outside the tensor: zeros)
+  // stage input in the padded point layout: each group of pg points walked
+  // with a box one point wider (the extra point is outside the tensor: zeros)
+  const int pg = s->ks.vPadG;
+  (void)n1;
   auto map_padded = [&](CUtensorMap *m, void *base) {
-    const cuuint64_t dims[4] = {L, (cuuint64_t)n1, (cuuint64_t)(nS / n1), (cuuint64_t)nV};
-    const cuuint64_t str[3] = {L * es, L * es * n1, L * es * nS};
-    const cuuint32_t box[4] = {te, (cuuint32_t)(n1 + 1), (cuuint32_t)(nS / n1), (cuuint32_t)nV};
+    const cuuint64_t dims[4] = {L, (cuuint64_t)pg, (cuuint64_t)(nS / pg), (cuuint64_t)nV};
+    const cuuint64_t str[3] = {L * es, L * es * pg, L * es * nS};
+    const cuuint32_t box[4] = {te, (cuuint32_t)(pg + 1), (cuuint32_t)(nS / pg), (cuuint32_t)nV};
     return make_map_nd(m, base, ts, es, 4, dims, str, box);
   };
   const CUtensorMapDataType f64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
@@ -1690,6 +1692,9 @@ struct AdjState {
   double *trY = nullptr, *fnbar = nullptr, *ybar = nullptr, *grad = nullptr, *part = nullptr;
   double *thetaBar = nullptr;
   double *thetaDir = nullptr;  // 5 doubles, device
+  // viscous runs: forward gradient, projected fluxes and the pass buffers of
+  // the viscous adjoint (AdjViscBufs)
+  double *vg = nullptr, *vfvn = nullptr, *vfvn2 = nullptr, *vub = nullptr, *vufb = nullptr, *vdcb = nullptr;
   double *ckpt = nullptr;    // (nCkpt + 1) states: U at steps 0, k, 2k, ... and U_N last
   double *stages = nullptr;  // k * nRK stage states of one segment
   // checkpointed runs: a second set of stage slots, so that the reverse sweep
@@ -1720,7 +1725,8 @@ void adj_free(frg_solver *s) {
   if (!a) return;
   for (auto &g : a->graphs) cudaGraphExecDestroy(g.second.exec);
   double *p[] = {a->seed[0], a->seed[1], a->lam[0], a->lam[1], a->trY, a->fnbar, a->ybar, a->grad, a->part,
-                 a->thetaBar, a->thetaDir, a->ckpt, a->stages, a->stages2};
+                 a->thetaBar, a->thetaDir, a->ckpt, a->stages, a->stages2, a->vg, a->vfvn, a->vfvn2, a->vub,
+                 a->vufb, a->vdcb};
   for (double *q : p) if (q) cudaFree(q);
   if (a->evFork) cudaEventDestroy(a->evFork);
   if (a->evJoin) cudaEventDestroy(a->evJoin);
@@ -1749,14 +1755,13 @@ frg_status adj_init(frg_solver *s) {
   if (s->adj) return FRG_OK;
   const frg_params &p = s->p;
   if (p.precision != FRG_FP64) return fail(FRG_ERR_ARG, "adjoint: FP64 precision only");
-  if (p.viscous) return fail(FRG_ERR_ARG, "adjoint: viscous flux not supported");
   if (!g_adj_tables[p.nDims - 2]) {
     cudaError_t e = p.nDims == 2 ? upload_tables_adj_2d() : upload_tables_adj_3d();
     if (e != cudaSuccess) return fail(FRG_ERR_CUDA, "adjoint tables: %s", cudaGetErrorString(e));
     g_adj_tables[p.nDims - 2] = true;
   }
   std::unique_ptr<AdjState> a(new AdjState);
-  KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType, 0};
+  KernelKey key{p.nDims, p.order, s->nV, p.precision, s->g.nBndFaces > 0 ? 1 : 0, p.riemannType, p.viscous ? 1 : 0};
   std::string err;
   const bool ok = p.nDims == 2 ? select_adj_2d(key, a->ks, err) : select_adj_3d(key, a->ks, err);
   if (!ok) return fail(FRG_ERR_ARG, "%s", err.c_str());
@@ -1766,7 +1771,10 @@ frg_status adj_init(frg_solver *s) {
   if ((st = dalloc(&a->seed[0], nSE)) || (st = dalloc(&a->seed[1], nSE)) || (st = dalloc(&a->lam[0], nSE)) ||
       (st = dalloc(&a->lam[1], nSE)) || (st = dalloc(&a->trY, nFE)) || (st = dalloc(&a->fnbar, nFE)) ||
       (st = dalloc(&a->ybar, nSE)) || (st = dalloc(&a->grad, nSE)) || (st = dalloc(&a->part, nPart)) ||
-      (st = dalloc(&a->thetaBar, 1)) || (st = dalloc(&a->thetaDir, 5))) {
+      (st = dalloc(&a->thetaBar, 1)) || (st = dalloc(&a->thetaDir, 5)) ||
+      (p.viscous && ((st = dalloc(&a->vg, (size_t)p.nDims * nSE)) || (st = dalloc(&a->vfvn, nFE)) ||
+                     (st = dalloc(&a->vfvn2, nFE)) || (st = dalloc(&a->vub, nSE)) || (st = dalloc(&a->vufb, nFE)) ||
+                     (st = dalloc(&a->vdcb, nFE))))) {
     s->adj = a.release();
     return st;
   }
@@ -1797,6 +1805,8 @@ AdjArgs adj_args(frg_solver *s, const double *Y, const double *gbar) {
   a.thetaDir = s->adj->thetaDir;
   a.grp = s->grp;
   a.dtGrp = s->grpDt;  // slot 0: the fixed per-group dt
+  a.v = AdjViscBufs{s->adj->vg, s->adj->vfvn, s->adj->vfvn2, s->adj->vub, s->adj->vufb, s->adj->vdcb,
+                    s->visc2 ? 1 : 0};
   a.ph = make_phys(s->p);
   return a;
 }
@@ -1806,6 +1816,7 @@ frg_status adj_launch(frg_solver *s, const AdjArgs &a) {
   frg_status st = post_launch(s);
   if (st) return st;
   s->adj->ks.elem(a, s->stream);
+  s->launches += s->adj->ks.elemLaunches - 1;
   return post_launch(s);
 }
 

@@ -68,16 +68,28 @@ struct Cfg {
   static constexpr int NF = 2 * DIM * NFF;
   static constexpr int NT = 256;  // threads per block
   // Shared-memory slot of solution point s in the per-point tile arrays.  In
-  // 3D one empty slot follows every coordinate line along xi, so the points
-  // that start the lines of a face (4 apart at P = 3) fall on different
-  // shared-memory banks instead of one (2D: no padding).
-  static constexpr int NSP = DIM == 3 ? NS + NS / N1 : NS;
+  // 3D one empty slot follows every PADG points -- by default every
+  // coordinate line along xi, so the points that start the lines of a face
+  // (4 apart at P = 3) fall on different shared-memory banks instead of one
+  // (2D: no padding).
+  static constexpr int PADG = N1;
+  static constexpr int NSP = DIM == 3 ? NS + NS / PADG : NS;
 };
 template <class C>
 __device__ __forceinline__ constexpr int sx(int s) {
-  if constexpr (C::DIM == 3) return s + s / C::N1;
+  if constexpr (C::DIM == 3) return s + s / C::PADG;
   else return s;
 }
+// The 3D tiles of 4 FP32 (2 FP64) elements of the TMA viscous kernels: a
+// warp spans 8 consecutive points, which one empty slot per 8 points keeps
+// on distinct banks in the point-wise and coordinate-line passes (one per xi
+// line would put points 0 and 7 on one bank); orders whose point count 8
+// does not divide keep the per-line padding.
+template <class C>
+struct CfgV : C {
+  static constexpr int PADG = C::NS % 8 == 0 ? 8 : C::N1;
+  static constexpr int NSP = C::NS + C::NS / PADG;
+};
 
 // Elements per block: as many as fit ~100 KB of shared memory (two blocks per
 // SM), capped at 32 so a warp spans 32 elements of one point.

@@ -98,7 +98,11 @@ struct VGradT {
   static constexpr int oNbr = oNrm + al(D * NF * TE * (int)sizeof(S));
   static constexpr int oBar = oNbr + al(NF * TE * 4);
   static constexpr int SMEM = oBar + 2 * 8 + 128;
-  static constexpr int MINB = SMEM * 3 <= 227 * 1024 ? (NT <= 128 ? 3 : 2) : SMEM * 2 <= 227 * 1024 ? 2 : 1;
+  // resident blocks per SM the register budget is sized for (meshes with
+  // boundary faces carry the ghost-state and wall code: two blocks)
+  static constexpr int minb(bool bc) {
+    return SMEM * 3 <= 227 * 1024 && (NT <= 128 || !bc) ? 3 : SMEM * 2 <= 227 * 1024 ? 2 : 1;
+  }
 };
 
 template <class C, typename R, typename S, int TE_, int NT_>
@@ -272,7 +276,7 @@ __device__ __forceinline__ void visc_point_gradient(const OpTab<R> &op, const R 
 // Pass 1: projected viscous flux of every flux point of the tile.
 // ----------------------------------------------------------------------------
 template <class C, typename R, typename S, bool BC, int TE, int NT>
-__global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::MINB))
+__global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
     fr_visc3_grad_tma_kernel(const StageArgs a, const __grid_constant__ ViscMaps m) {
   static_assert(C::DIM == 3 && sizeof(R) == sizeof(S), "3D, compute type = stored type");
   using T = VGradT<C, R, S, TE, NT>;

@@ -149,7 +149,7 @@ bool make_set(KernelSet &k, std::string &err) {
 // per SM), 256 for the stage pass (two blocks per SM, by shared memory)
 template <typename S>
 constexpr int visc_tma_te() { return sizeof(S) == 4 ? 4 : 2; }
-constexpr int kViscGradNT = 128, kViscStageNT = 256;
+constexpr int kViscGradNT = 256, kViscStageNT = 256;
 template <class C, typename R, typename S, bool BC>
 void launch_visc3_grad(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
   fr_visc3_grad_tma_kernel<C, R, S, BC, visc_tma_te<S>(), kViscGradNT><<<nBlk, kViscGradNT, smem, st>>>(
@@ -160,8 +160,9 @@ void launch_visc3_stage(const void *args, const void *maps, int nBlk, size_t sme
   fr_visc3_stage_tma_kernel<C, R, S, BC, RS, visc_tma_te<S>(), kViscStageNT><<<nBlk, kViscStageNT, smem, st>>>(
       *static_cast<const StageArgs *>(args), *static_cast<const ViscMaps *>(maps));
 }
-template <class C, typename R, typename S, bool BC, int RS>
+template <class C0, typename R, typename S, bool BC, int RS>
 cudaError_t add_visc3_tma(KernelSet &k) {
+  using C = CfgV<C0>;  // the TMA tiles' point padding
   constexpr int TE = visc_tma_te<S>();
   using TG = VGradT<C, R, S, TE, kViscGradNT>;
   using TS = VStageT<C, R, S, TE, kViscStageNT>;
@@ -178,6 +179,7 @@ cudaError_t add_visc3_tma(KernelSet &k) {
   k.vgrad = &launch_visc3_grad<C, R, S, BC>;
   k.vstage = &launch_visc3_stage<C, R, S, BC, RS>;
   k.vTE = TE;
+  k.vPadG = C::PADG;
   k.vgradSmem = TG::SMEM;
   k.vstageSmem = TS::SMEM;
   return cudaSuccess;

@@ -244,3 +244,102 @@ def test_checkpointed_and_stored_sweeps_agree():
         # the overlapped recompute / reverse) and must give the same bits
         assert np.array_equal(s.adjoint_backward(None, np.array([0.0, c, 0, 0, 0]))[0], out[-1])
     assert relerr(out[1], out[0]) < 1e-12 and relerr(out[2], out[0]) < 1e-12
+
+
+# ---- viscous (LDG) residuals: the three-pass viscous adjoint
+def _visc_cases():
+    from fr_learn_b200 import box2d, box3d, bump2d
+
+    c = np.sqrt(GAMMA)
+    ns = dict(viscous=1, mu_inf=0.05, prandtl=0.72, fixVis=1, tau=1.0)
+    return {
+        "ns2d_p3_roe_periodic": (box2d(4, 4, -5, 5, -5, 5, perturb=0.1, seed=13), 1,
+                                 dict(order=3, riemannType=1, penFact=0.5, **ns)),
+        "ns2d_p2_walls_char": (bump2d(5, 3, bc_wall="adiabatic_noslip", bc_top="isothermal_noslip"), 0,
+                               dict(order=2, riemannType=0, penFact=0.3, TWall=1.0, RGas=1.0 / GAMMA,
+                                    uBound=0.3 * c, pBound=1.0, **ns)),
+        "ns2d_p2_sutherland_slip": (bump2d(5, 3), 0,
+                                    dict(order=2, riemannType=1, penFact=0.0, uBound=0.4 * c, pBound=1.0,
+                                         viscous=1, mu_inf=0.05, prandtl=0.71, fixVis=0, c_sth=0.41, rt_inf=2.5,
+                                         tau=1.0)),
+        "ns3d_p2_periodic": (box3d(3, 3, 3, (0, 0, 0), (2 * np.pi,) * 3, perturb=0.05, seed=14), 10,
+                             dict(order=2, penFact=0.0, **ns)),
+        "ns3d_p2_penalty_walls": (box3d(3, 3, 3, (-2, -2, -1), (2, 2, 1),
+                                        bcs={"zmin": "adiabatic_noslip", "zmax": "isothermal_noslip"},
+                                        perturb=0.1, seed=15), 1,
+                                  dict(order=2, penFact=0.3, TWall=1.0, RGas=1.0 / GAMMA, **ns)),
+        "advdiff2d_p3": (box2d(4, 4, perturb=0.1, seed=16), 0,
+                         dict(order=3, equation=0, viscous=1, diffD=0.05, penFact=0.2, tau=1.0)),
+    }
+
+
+@pytest.mark.parametrize("name", list(_visc_cases().keys()))
+def test_viscous_residual_vjp_matches_central_differences(name):
+    mesh, ic, kw = _visc_cases()[name]
+    rng = np.random.default_rng(11)
+    s = _solver(mesh, ic, **kw) if ic != 10 else None
+    if s is None:
+        from fr_learn_b200 import Solver
+
+        s = Solver(mesh, dtType=0, dt=1e-3, **kw)
+        s.setInitialCondition(10, 0.2)
+    U = _perturbed_state(s, rng)
+    gbar = rng.standard_normal(U.shape)
+    delta = rng.standard_normal(U.shape) * np.abs(U).max(axis=(0, 1), keepdims=True)
+    s.set("U_spts", U)
+    theta = None
+    if "char" in name or "slip" in name:
+        theta = np.array([0.0, np.sqrt(GAMMA), 0.0, 0.0, 0.0])  # d(u_B)/dMach
+    ubar, tbar = s.residual_vjp(gbar, theta)
+    eps = 1e-6
+    fd = np.sum(gbar * (_residual(s, U + eps * delta) - _residual(s, U - eps * delta))) / (2 * eps)
+    adj = np.sum(ubar * delta)
+    bound = np.linalg.norm(ubar) * np.linalg.norm(delta)
+    assert abs(fd - adj) <= 1e-6 * abs(adj) + 1e-10 * bound, (fd, adj, bound)
+    if theta is not None:
+        M = kw["uBound"] / np.sqrt(GAMMA)
+        R = []
+        for sg in (1, -1):
+            k2 = dict(kw, uBound=(M + sg * eps) * np.sqrt(GAMMA))
+            s2 = _solver(mesh, ic, **k2)
+            R.append(_residual(s2, U))
+        fdt = np.sum(gbar * (R[0] - R[1])) / (2 * eps)
+        assert abs(fdt - tbar) <= 1e-5 * max(abs(tbar), 1e-8), (fdt, tbar)
+
+
+@pytest.mark.parametrize("every", [3, 0])
+def test_viscous_adjoint_rk_matches_central_differences(every):
+    """Navier-Stokes channel over the bump (P = 2, Rusanov, LDG with a
+    penalty, adiabatic lower wall, isothermal top, characteristic in / out),
+    J = entropy-error integral after 6 RK4 steps: dJ/dU_0 along a random
+    direction and dJ/dMach against central differences of the forward solver."""
+    from fr_learn_b200 import bump2d
+
+    c = np.sqrt(GAMMA)
+    M = 0.3
+    mesh = bump2d(6, 3, bc_wall="adiabatic_noslip", bc_top="isothermal_noslip")
+    kw = dict(order=2, riemannType=0, viscous=1, mu_inf=0.05, prandtl=0.72, fixVis=1, tau=1.0, penFact=0.3,
+              TWall=1.0, RGas=1.0 / GAMMA, uBound=M * c, pBound=1.0, timeType=4)
+    nsteps = 6
+    rng = np.random.default_rng(5)
+    s = _solver(mesh, 0, **kw)
+    U0 = _perturbed_state(s, rng, amp=2e-3)
+    s.set("U_spts", U0)
+    s.adjoint_forward(nsteps, every)
+    J, _ = s.objective("entropy")
+    theta = np.array([0.0, c, 0.0, 0.0, 0.0])
+    lam0, tbar = s.adjoint_backward(None, theta)
+
+    def J_of(U, Mach):
+        s2 = _solver(mesh, 0, **dict(kw, uBound=Mach * c))
+        s2.set("U_spts", U)
+        s2.update(nsteps)
+        return s2.objective("entropy")[0]
+
+    eps = 1e-6
+    d = rng.standard_normal(U0.shape) * np.abs(U0).max(axis=(0, 1), keepdims=True)
+    fd = (J_of(U0 + eps * d, M) - J_of(U0 - eps * d, M)) / (2 * eps)
+    adj = float(np.sum(lam0 * d))
+    assert abs(fd - adj) <= 1e-5 * abs(adj), (fd, adj)
+    fdm = (J_of(U0, M + eps) - J_of(U0, M - eps)) / (2 * eps)
+    assert abs(fdm - tbar) <= 1e-5 * abs(fdm), (fdm, tbar)
