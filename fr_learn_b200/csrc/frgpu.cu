@@ -246,6 +246,7 @@ struct frg_solver {
   bool dtFresh = false;  // device dt was computed from the current wave speeds
   // tensor maps of the TMA stage kernel
   bool useTma = false;
+  bool pdl = true;  // programmatic dependent launch between TMA stages (FRG_PDL=0: off)
   int tmaVar = 0;  // tile-shape variant of the TMA kernel (frg_autotune)
   int nBlkTma = 0;
   CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
@@ -647,6 +648,9 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       a.divF = s->divF[0];
     }
     if (last && fused_dt(s)) a.flags |= SF_DTNEXT;
+    // stages after the first follow a stage kernel directly: programmatic
+    // dependent launch (not when each launch is timed on its own)
+    if (k > 0 && s->pdl && !ev) a.flags |= SF_PDL;
     if (s->useViscTma) {
       ViscMaps vm;
       vm.Uin = first ? s->vm.U : s->vm.Win[(k - 1) & 1];
@@ -824,6 +828,8 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     const char *env = getenv("FRG_KERNEL");
     s->useTma = !(env && std::strcmp(env, "generic") == 0);
     if (s->useTma && (st = setup_tma(s.get()))) return st;
+    const char *pe = getenv("FRG_PDL");
+    s->pdl = !(pe && std::strcmp(pe, "0") == 0);
   }
   if (s->ks.vgrad) {
     const char *env = getenv("FRG_KERNEL");

@@ -160,7 +160,8 @@ enum : int {
   SF_JAMESON = 16,  // timeType 5: every stage U = U0 - a t
   SF_TIME = 32,     // advance the device time by dt (block 0)
   SF_DIVF = 64,     // also store divF (residual monitoring) during an update
-  SF_DTNEXT = 128   // last stage: compute the next step's CFL dt (TMA kernel)
+  SF_DTNEXT = 128,  // last stage: compute the next step's CFL dt (TMA kernel)
+  SF_PDL = 256      // launch as a programmatic dependent of the previous kernel (host side)
 };
 
 // Arguments of one stage launch.  Arrays of the stored type S (double, or

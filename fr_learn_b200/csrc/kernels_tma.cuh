@@ -88,6 +88,18 @@ __device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Programmatic dependent launch.  Launched with the programmatic-
+// serialization attribute, a stage kernel's blocks may start while the
+// previous stage's last blocks still run; they issue the loads of the
+// read-only metric tiles, then wait (pdl_wait) until the previous grid has
+// finished and its writes are visible before touching anything a stage
+// writes.  Each block signals at its start that the next stage may be
+// scheduled (it is, once every block of this grid has signalled or exited).
+// Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Tile of the TMA kernel: TE elements (box inner extent TE * sizeof >= 16 B),
 // NT threads.  TE_ = 0 picks the widest of 16/8/4 elements whose shared
@@ -154,26 +166,33 @@ struct TmaNeeds {
   }
 };
 
-// One thread: every bulk tensor load of the tile starting at element e0,
-// in three groups on bar[0..2] (see the file comment).
+// One thread: the bulk tensor loads of the tile starting at element e0, in
+// three groups on bar[0..2] (see the file comment).  part 1: every group's
+// expected byte count and the read-only metric tiles; part 2: the tiles a
+// previous stage writes (state, traces, U0, accumulator); both parts when
+// part is 0.
 template <class C, typename R, typename S, int TE>
 __device__ __forceinline__ void tma_issue_tile(const TmaMaps &m, const TmaNeeds &nd, const TmaBufs<R, S> &b, int e0,
-                                               uint64_t *bar) {
+                                               uint64_t *bar, int part = 0) {
   constexpr int NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM;
-  const uint32_t b0 = (nd.inU ? NV * NS * TE * 8 : NV * NS * TE * (int)sizeof(S)) + DIM * DIM * NS * TE * sizeof(S) +
-                      NF * TE * 4;
-  mbar_expect_tx(&bar[0], b0);
+  if (part != 2) {
+    const uint32_t b0 = (nd.inU ? NV * NS * TE * 8 : NV * NS * TE * (int)sizeof(S)) +
+                        DIM * DIM * NS * TE * sizeof(S) + NF * TE * 4;
+    mbar_expect_tx(&bar[0], b0);
+    mbar_expect_tx(&bar[1], (DIM * NF * TE + NF * TE + NV * NF * TE) * sizeof(S));
+    const uint32_t b2 =
+        NS * TE * sizeof(S) + (nd.needU0 ? NV * NS * TE * 8 : 0) + (nd.needAcc ? NV * NS * TE * 8 : 0);
+    mbar_expect_tx(&bar[2], b2);
+    tma_load2d(b.JG, &m.JG, e0, 0, &bar[0]);
+    tma_load2d(b.Nbr, &m.nbr, e0, 0, &bar[0]);
+    tma_load2d(b.Nrm, &m.nrm, e0, 0, &bar[1]);
+    tma_load2d(b.DA, &m.dA, e0, 0, &bar[1]);
+    tma_load2d(b.Det, &m.det, e0, 0, &bar[2]);
+  }
+  if (part == 1) return;
   if (nd.inU) tma_load2d(b.U0, &m.U, e0, 0, &bar[0]);
   else tma_load2d(b.Us, &m.Win, e0, 0, &bar[0]);
-  tma_load2d(b.JG, &m.JG, e0, 0, &bar[0]);
-  tma_load2d(b.Nbr, &m.nbr, e0, 0, &bar[0]);
-  mbar_expect_tx(&bar[1], (DIM * NF * TE + NF * TE + NV * NF * TE) * sizeof(S));
-  tma_load2d(b.Nrm, &m.nrm, e0, 0, &bar[1]);
-  tma_load2d(b.DA, &m.dA, e0, 0, &bar[1]);
   tma_load2d(b.Tw, &m.trIn, e0, 0, &bar[1]);
-  const uint32_t b2 = NS * TE * sizeof(S) + (nd.needU0 ? NV * NS * TE * 8 : 0) + (nd.needAcc ? NV * NS * TE * 8 : 0);
-  mbar_expect_tx(&bar[2], b2);
-  tma_load2d(b.Det, &m.det, e0, 0, &bar[2]);
   if (nd.needU0) tma_load2d(b.U0, &m.U, e0, 0, &bar[2]);
   if (nd.needAcc) tma_load2d(b.Acc, &m.Acc, e0, 0, &bar[2]);
 }
@@ -475,7 +494,10 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
     fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, b, e0, bar);
+  pdl_launch_dependents();
+  if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, b, e0, bar, 1);
+  pdl_wait();  // the previous stage has finished: its outputs are visible
+  if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, b, e0, bar, 2);
 
   // the global dt, fetched while the tiles are in flight
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
@@ -625,7 +647,10 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
     fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, slot(0), blockIdx.x * TE, &bar[0]);
+  pdl_launch_dependents();
+  if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, slot(0), blockIdx.x * TE, &bar[0], 1);
+  pdl_wait();  // the previous stage has finished: its outputs are visible
+  if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, slot(0), blockIdx.x * TE, &bar[0], 2);
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   double dtMin = INFINITY;
   const bool dtn = flags & SF_DTNEXT;
@@ -809,18 +834,23 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
 
   // thread 0: a tile's ring groups (0: stage input W, JGinv, codes; 1:
   // normals, dA, own traces; 2: 1/detJ) into slot k
-  auto issue_slot = [&](const TmaBufs<R, S> &b, int e0, uint64_t *bk) {
-    mbar_expect_tx(&bk[0], (nd.inU ? 0u : (uint32_t)(NV * NS * TE * sizeof(S))) +
-                               (uint32_t)(DIM * DIM * NS * TE * sizeof(S)) + (uint32_t)(NF * TE * 4));
+  // (part 1: the byte counts and the read-only metric tiles; part 2: the
+  // stage input and traces a previous stage writes; 0: both)
+  auto issue_slot = [&](const TmaBufs<R, S> &b, int e0, uint64_t *bk, int part) {
+    if (part != 2) {
+      mbar_expect_tx(&bk[0], (nd.inU ? 0u : (uint32_t)(NV * NS * TE * sizeof(S))) +
+                                 (uint32_t)(DIM * DIM * NS * TE * sizeof(S)) + (uint32_t)(NF * TE * 4));
+      mbar_expect_tx(&bk[1], (uint32_t)((DIM * NF * TE + NF * TE + NV * NF * TE) * sizeof(S)));
+      mbar_expect_tx(&bk[2], (uint32_t)(NS * TE * sizeof(S)));
+      tma_load2d(b.JG, &m.JG, e0, 0, &bk[0]);
+      tma_load2d(b.Nbr, &m.nbr, e0, 0, &bk[0]);
+      tma_load2d(b.Nrm, &m.nrm, e0, 0, &bk[1]);
+      tma_load2d(b.DA, &m.dA, e0, 0, &bk[1]);
+      tma_load2d(b.Det, &m.det, e0, 0, &bk[2]);
+    }
+    if (part == 1) return;
     if (!nd.inU) tma_load2d(b.Us, &m.Win, e0, 0, &bk[0]);
-    tma_load2d(b.JG, &m.JG, e0, 0, &bk[0]);
-    tma_load2d(b.Nbr, &m.nbr, e0, 0, &bk[0]);
-    mbar_expect_tx(&bk[1], (uint32_t)((DIM * NF * TE + NF * TE + NV * NF * TE) * sizeof(S)));
-    tma_load2d(b.Nrm, &m.nrm, e0, 0, &bk[1]);
-    tma_load2d(b.DA, &m.dA, e0, 0, &bk[1]);
     tma_load2d(b.Tw, &m.trIn, e0, 0, &bk[1]);
-    mbar_expect_tx(&bk[2], (uint32_t)(NS * TE * sizeof(S)));
-    tma_load2d(b.Det, &m.det, e0, 0, &bk[2]);
   };
   // thread 0: the tile's double stage input or U0 (barU), and its RK
   // accumulator (barA), into the block's FP64 buffers
@@ -839,8 +869,11 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     fence_mbar_init();
   }
   __syncthreads();
+  pdl_launch_dependents();
+  if (tid == 0) issue_slot(slot(0), blockIdx.x * TE, &bar[0], 1);
+  pdl_wait();  // the previous stage has finished: its outputs are visible
   if (tid == 0) {
-    issue_slot(slot(0), blockIdx.x * TE, &bar[0]);
+    issue_slot(slot(0), blockIdx.x * TE, &bar[0], 2);
     if (needUg) issue_u(slot(0), blockIdx.x * TE);
   }
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
@@ -887,7 +920,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     if (tid == 0) {
       const int tn = t + gridDim.x;
       if (tn < nTiles) {
-        issue_slot(slot(k ^ 1), tn * TE, &bar[3 * (k ^ 1)]);
+        issue_slot(slot(k ^ 1), tn * TE, &bar[3 * (k ^ 1)], 0);
         sIss++;
       }
     }

@@ -16,10 +16,28 @@ template <class C, typename R, typename S, bool BC, int RS>
 void launch_stage(const void *args, int nBlk, size_t smem, cudaStream_t st) {
   fr_stage_kernel<C, R, S, BC, RS><<<nBlk, C::NT, smem, st>>>(*static_cast<const StageArgs *>(args));
 }
+// A TMA stage kernel's launch; with SF_PDL it is a programmatic dependent of
+// the previous kernel in the stream (its blocks may start while that kernel's
+// last blocks run, see pdl_wait).
+template <class K>
+void launch_tma_stage(K kernel, const void *args, const void *maps, int nBlk, int nt, size_t smem, cudaStream_t st) {
+  const StageArgs &a = *static_cast<const StageArgs *>(args);
+  const TmaMaps &m = *static_cast<const TmaMaps *>(maps);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(nBlk);
+  cfg.blockDim = dim3(nt);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = (a.flags & SF_PDL) ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, a, m);
+}
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 void launch_stage_tma(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
-  fr_stage_tma_kernel<C, R, S, BC, RS, TEV, NTV><<<nBlk, NTV, smem, st>>>(*static_cast<const StageArgs *>(args),
-                                                                          *static_cast<const TmaMaps *>(maps));
+  launch_tma_stage(fr_stage_tma_kernel<C, R, S, BC, RS, TEV, NTV>, args, maps, nBlk, NTV, smem, st);
 }
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 cudaError_t add_tma_variant(KernelSet &k) {
@@ -38,8 +56,7 @@ cudaError_t add_tma_variant(KernelSet &k) {
 }
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV, int NB>
 void launch_stage_pipe(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
-  fr_stage_tma_pipe_kernel<C, R, S, BC, RS, TEV, NTV, NB><<<nBlk, NTV, smem, st>>>(
-      *static_cast<const StageArgs *>(args), *static_cast<const TmaMaps *>(maps));
+  launch_tma_stage(fr_stage_tma_pipe_kernel<C, R, S, BC, RS, TEV, NTV, NB>, args, maps, nBlk, NTV, smem, st);
 }
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV, int NB>
 cudaError_t add_pipe_variant(KernelSet &k) {
@@ -61,8 +78,7 @@ cudaError_t add_pipe_variant(KernelSet &k) {
 }
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 void launch_stage_split(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) {
-  fr_stage_tma_split_kernel<C, R, S, BC, RS, TEV, NTV><<<nBlk, NTV, smem, st>>>(
-      *static_cast<const StageArgs *>(args), *static_cast<const TmaMaps *>(maps));
+  launch_tma_stage(fr_stage_tma_split_kernel<C, R, S, BC, RS, TEV, NTV>, args, maps, nBlk, NTV, smem, st);
 }
 template <class C, typename R, typename S, bool BC, int RS, int TEV, int NTV>
 cudaError_t add_split_variant(KernelSet &k) {
