@@ -125,9 +125,9 @@ __global__ void __launch_bounds__(256) fr_adj_face_kernel(const AdjArgs a) {
 template <class C>
 struct AdjTile {
   static constexpr int PER_ELE = (2 * C::NV * C::NS + 2 * C::NV * C::NF) * 8;
-  // at most 8 elements per block: the dual-number Jacobians hold ~255
-  // registers per thread (two blocks per SM), so small tiles keep every SM
-  // busy on meshes of a few thousand elements
+  // at most 8 elements per block: the dual-number Jacobians need many
+  // registers (capped for three blocks per SM), so small tiles keep every
+  // SM busy on meshes of a few thousand elements
   static constexpr int TE = (8 * PER_ELE <= 64 * 1024) ? 8 : (4 * PER_ELE <= 64 * 1024) ? 4
                             : (2 * PER_ELE <= 64 * 1024) ? 2 : 1;
   static constexpr int NT = 128;
@@ -136,7 +136,7 @@ struct AdjTile {
 
 // Element pass: one block per tile of TE elements.
 template <class C, bool BC, int RS>
-__global__ void __launch_bounds__(128) fr_adj_elem_kernel(const AdjArgs a) {
+__global__ void __launch_bounds__(128, 3) fr_adj_elem_kernel(const AdjArgs a) {
   using T = AdjTile<C>;
   constexpr int TE = T::TE, NT = T::NT, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1;
   using D1 = ad::Dual<NV + 1>;  // own trace + the freestream parameter

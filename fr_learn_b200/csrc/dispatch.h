@@ -47,6 +47,9 @@ struct KernelSet {
   void (*vstage)(const void *args, const void *maps, int nBlk, size_t smem, cudaStream_t st) = nullptr;
   int vTE = 0;
   int vPadG = 0;  // points per padding slot of their tiles' point layout
+  // resident blocks per SM of the two passes (their grids are persistent:
+  // at most SMs x this many blocks, each walking tiles)
+  int vgradOcc = 0, vstageOcc = 0;
   size_t vgradSmem = 0, vstageSmem = 0;
 };
 

@@ -247,6 +247,7 @@ struct frg_solver {
   // tensor maps of the TMA stage kernel
   bool useTma = false;
   bool pdl = true;  // programmatic dependent launch between TMA stages (FRG_PDL=0: off)
+  int nSM = 0;      // multiprocessors of the device (persistent grids)
   int tmaVar = 0;  // tile-shape variant of the TMA kernel (frg_autotune)
   int nBlkTma = 0;
   CUtensorMap mU, mAcc, mW[2], mTr[2], mJG, mDet, mNrm, mDA, mNbr;
@@ -665,10 +666,10 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       vm.nbr = s->vm.nbr;
       vm.fvn = s->vm.fvn;
       vm.fvn2 = s->vm.fvn2;
-      const int nBlk = (s->nE + s->ks.vTE - 1) / s->ks.vTE;
-      s->ks.vgrad(&a, &vm, nBlk, s->ks.vgradSmem, s->stream);
+      const int nTiles = (s->nE + s->ks.vTE - 1) / s->ks.vTE;
+      s->ks.vgrad(&a, &vm, std::min(nTiles, s->nSM * s->ks.vgradOcc), s->ks.vgradSmem, s->stream);
       if ((st = post_launch(s))) return st;
-      s->ks.vstage(&a, &vm, nBlk, s->ks.vstageSmem, s->stream);
+      s->ks.vstage(&a, &vm, std::min(nTiles, s->nSM * s->ks.vstageOcc), s->ks.vstageSmem, s->stream);
       st = post_launch(s);
     } else if (s->useTma) {
       TmaMaps mm;
@@ -831,6 +832,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     const char *pe = getenv("FRG_PDL");
     s->pdl = !(pe && std::strcmp(pe, "0") == 0);
   }
+  CK(cudaDeviceGetAttribute(&s->nSM, cudaDevAttrMultiProcessorCount, dev));
   if (s->ks.vgrad) {
     const char *env = getenv("FRG_KERNEL");
     s->useViscTma = !(env && std::strcmp(env, "generic") == 0);

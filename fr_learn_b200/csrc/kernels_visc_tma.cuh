@@ -64,6 +64,19 @@ __device__ __forceinline__ void tma_load4d(void *dst, const CUtensorMap *m, int 
       "l"(m), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(b))
       : "memory");
 }
+// L2 prefetch of a tensor tile (no shared memory involved)
+__device__ __forceinline__ void tma_prefetch2d(const CUtensorMap *m, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(m), "r"(x), "r"(y) : "memory");
+}
+__device__ __forceinline__ void tma_prefetch3d(const CUtensorMap *m, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(m), "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+__device__ __forceinline__ void tma_prefetch4d(const CUtensorMap *m, int x, int y, int z, int w) {
+  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(m), "r"(x), "r"(y),
+               "r"(z), "r"(w)
+               : "memory");
+}
 __device__ __forceinline__ void tma_store3d(const CUtensorMap *m, int x, int y, int z, const void *src) {
   asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(m),
                "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
@@ -296,9 +309,10 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
   S *FvO = reinterpret_cast<S *>(Dc);   // output after the gradient has read Dc
   S *Fv2 = reinterpret_cast<S *>(Ntr);  // penalty projection after the LDG phase has read Ntr
   const OpTab<R> &op = optab<R>(a.vcjh, C::P);
-  const int tid = threadIdx.x, e0 = blockIdx.x * TE;
+  const int tid = threadIdx.x, nTiles = (a.nEle + TE - 1) / TE;
   const bool inU = a.Uin_d != nullptr;
-  bool ok;
+  bool ok = true;
+  uint32_t par = 0;
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -306,7 +320,13 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
     fence_mbar_init();
   }
   __syncthreads();
+  // persistent: the block walks tiles blockIdx.x, + gridDim.x, ...; each
+  // tile's inputs are prefetched into L2 one tile ahead
+  for (int t = blockIdx.x, j = 0; t < nTiles; t += gridDim.x, j++) {
+  const int e0 = t * TE;
+  par = (uint32_t)(j & 1);
   if (tid == 0) {
+    tma_wait_reads();  // the previous tile's stores have read shared memory
     const uint32_t bst = inU ? (uint32_t)(NV * NS * TE * 8) : (uint32_t)(NV * NSP * TE * sizeof(S));
     mbar_expect_tx(&bar[0], bst + (uint32_t)((nbr_by_tma<TE>() ? NF * TE * 4 : 0) + DIM * NF * TE * sizeof(S)));
     if (inU) tma_load3d(Stg, &m.Uin, e0, 0, 0, &bar[0]);
@@ -316,16 +336,26 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
     mbar_expect_tx(&bar[1], (uint32_t)((DIM * DIM * NS * TE + NS * TE) * sizeof(S)));
     tma_load3d(JG, &m.JG, e0, 0, 0, &bar[1]);
     tma_load2d(Det, &m.det, e0, 0, &bar[1]);
+    const int tn = t + gridDim.x;
+    if (tn < nTiles) {
+      const int en = tn * TE;
+      if (inU) tma_prefetch3d(&m.Uin, en, 0, 0);
+      else tma_prefetch4d(&m.Uin, en, 0, 0, 0);
+      if constexpr (nbr_by_tma<TE>()) tma_prefetch2d(&m.nbr, en, 0);
+      tma_prefetch3d(&m.nrm, en, 0, 0);
+      tma_prefetch3d(&m.JG, en, 0, 0);
+      tma_prefetch2d(&m.det, en, 0);
+    }
   }
   if constexpr (!nbr_by_tma<TE>()) load_nbr_plain<C, TE, NT>(a, Nbr, e0);
-  ok = mbar_wait(&bar[0], 0);
+  ok = mbar_wait(&bar[0], par);
   if (__syncthreads_or(!ok)) goto timeout;
   visc_gather<C, S, TE, NT>(a, a.trIn, Nbr, Ntr, e0);
   if (inU) visc_convert_input<C, R, TE, NT>(Stg, Us);
   cp_async_wait_all();
   __syncthreads();
   visc_ldg<C, R, S, BC, TE, NT>(a, op, Us, Ntr, Nrm, Nbr, Dc, e0);
-  ok = mbar_wait(&bar[1], 0);
+  ok = mbar_wait(&bar[1], par);
   if (__syncthreads_or(!ok)) goto timeout;
   // corrected gradient at the solution points (calcGradU_spts, correctGradU)
   for (int it = tid; it < NS * TE; it += NT) {
@@ -393,14 +423,16 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
     tma_store3d(&m.fvn, e0, 0, 0, FvO);
     if (a.visc2) tma_store3d(&m.fvn2, e0, 0, 0, Fv2);
     tma_commit();
-    tma_wait_reads();
   }
+  }  // tiles
+  if (tid == 0) tma_wait_reads();
   return;
 
 timeout:
   if (tid == 0) {
     atomicOr(a.err, ERRF_TIMEOUT);
-    for (int i = 0; i < 2; i++) mbar_wait(&bar[i], 0);  // bounded: let copies in flight land
+    for (int i = 0; i < 2; i++) mbar_wait(&bar[i], par);  // bounded: let copies in flight land
+    tma_wait_reads();
   }
   cp_async_wait_all();
   __syncthreads();
@@ -436,18 +468,26 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   S *Wst = reinterpret_cast<S *>(JG);     // new stage state, after the fluxes have read JG
   S *TrO = reinterpret_cast<S *>(Ntr);    // new traces, after phase B has read Ntr
   const OpTab<R> &op = optab<R>(a.vcjh, C::P);
-  const int tid = threadIdx.x, e0 = blockIdx.x * TE, flags = a.flags;
+  const int tid = threadIdx.x, flags = a.flags, nTiles = (a.nEle + TE - 1) / TE;
   const bool last = flags & SF_LAST, first = flags & SF_FIRST, jam = flags & SF_JAMESON;
   const TmaNeeds nd(a);
   const Phys &ph = a.ph;
-  bool ok;
+  bool ok = true;
+  uint32_t par = 0;
 
   if (tid == 0) {
     for (int i = 0; i < 3; i++) mbar_init(&bar[i], 1);
     fence_mbar_init();
   }
   __syncthreads();
+  const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
+  // persistent: the block walks tiles blockIdx.x, + gridDim.x, ...; each
+  // tile's inputs are prefetched into L2 one tile ahead
+  for (int t = blockIdx.x, j = 0; t < nTiles; t += gridDim.x, j++) {
+  const int e0 = t * TE;
+  par = (uint32_t)(j & 1);
   if (tid == 0) {
+    tma_wait_reads();  // the previous tile's stores have read shared memory
     const uint32_t bst = nd.inU ? (uint32_t)(NV * NS * TE * 8) : (uint32_t)(NV * NSP * TE * sizeof(S));
     mbar_expect_tx(&bar[0], bst + (uint32_t)(nbr_by_tma<TE>() ? NF * TE * 4 : 0) +
                                 (uint32_t)((DIM * NF * TE + DIM * DIM * NS * TE + NS * TE) * sizeof(S)));
@@ -463,11 +503,24 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
     mbar_expect_tx(&bar[2], (uint32_t)((nd.needU0 ? NV * NS * TE * 8 : 0) + (nd.needAcc ? NV * NS * TE * 8 : 0)));
     if (nd.needU0) tma_load3d(U0, &m.U, e0, 0, 0, &bar[2]);
     if (nd.needAcc) tma_load3d(Acc, &m.Acc, e0, 0, 0, &bar[2]);
+    const int tn = t + gridDim.x;
+    if (tn < nTiles) {
+      const int en = tn * TE;
+      if (nd.inU) tma_prefetch3d(&m.Uin, en, 0, 0);
+      else tma_prefetch4d(&m.Uin, en, 0, 0, 0);
+      if constexpr (nbr_by_tma<TE>()) tma_prefetch2d(&m.nbr, en, 0);
+      tma_prefetch3d(&m.nrm, en, 0, 0);
+      tma_prefetch3d(&m.JG, en, 0, 0);
+      tma_prefetch2d(&m.det, en, 0);
+      tma_prefetch2d(&m.dA, en, 0);
+      tma_prefetch3d(&m.fvn, en, 0, 0);
+      if (nd.needU0) tma_prefetch3d(&m.U, en, 0, 0);
+      if (nd.needAcc) tma_prefetch3d(&m.Acc, en, 0, 0);
+    }
   }
-  const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   if constexpr (!nbr_by_tma<TE>()) load_nbr_plain<C, TE, NT>(a, Nbr, e0);
 
-  ok = mbar_wait(&bar[0], 0);
+  ok = mbar_wait(&bar[0], par);
   if (__syncthreads_or(!ok)) goto timeout;
   visc_gather<C, S, TE, NT>(a, a.trIn, Nbr, Ntr, e0);
   visc_gather<C, S, TE, NT>(a, a.fvnIn, Nbr, Fn, e0);
@@ -509,7 +562,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
         Fs[((d1 * NV + v) * NSP + sx<C>(s)) * TE + e] = t;
       }
   }
-  ok = mbar_wait(&bar[1], 0);
+  ok = mbar_wait(&bar[1], par);
   if (__syncthreads_or(!ok)) goto timeout;
 
   // ---- B: common inviscid + LDG viscous flux and the jumps
@@ -588,7 +641,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
       Js[(v * NF + f) * TE + e] = fo - dis[v];
     }
   }
-  ok = mbar_wait(&bar[2], 0);
+  ok = mbar_wait(&bar[2], par);
   if (__syncthreads_or(!ok)) goto timeout;
 
   // ---- C: divergence + correction, the RK update (timeStepA/B) in FP64
@@ -642,7 +695,6 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
       Us[(v * NSP + sx<C>(s)) * TE + e] = (R)(last ? unew : (double)(S)unew);
     }
   }
-  if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
   fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
@@ -668,14 +720,17 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   if (tid == 0) {
     tma_store3d(&m.trOut, e0, 0, 0, TrO);
     tma_commit();
-    tma_wait_reads();
   }
+  }  // tiles
+  if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
+  if (tid == 0) tma_wait_reads();
   return;
 
 timeout:
   if (tid == 0) {
     atomicOr(a.err, ERRF_TIMEOUT);
-    for (int i = 0; i < 3; i++) mbar_wait(&bar[i], 0);  // bounded: let copies in flight land
+    for (int i = 0; i < 3; i++) mbar_wait(&bar[i], par);  // bounded: let copies in flight land
+    tma_wait_reads();
   }
   cp_async_wait_all();
   __syncthreads();

@@ -192,6 +192,10 @@ cudaError_t add_visc3_tma(KernelSet &k) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fs, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k.vgradOcc, fg, kViscGradNT, TG::SMEM);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k.vstageOcc, fs, kViscStageNT, TS::SMEM);
+  if (e != cudaSuccess) return e;
+  if (k.vgradOcc < 1 || k.vstageOcc < 1) return cudaErrorInvalidConfiguration;
   k.vgrad = &launch_visc3_grad<C, R, S, BC>;
   k.vstage = &launch_visc3_stage<C, R, S, BC, RS>;
   k.vTE = TE;
