@@ -126,17 +126,20 @@ template <class C>
 struct AdjTile {
   static constexpr int PER_ELE = (2 * C::NV * C::NS + 2 * C::NV * C::NF) * 8;
   // at most 8 elements per block: the dual-number Jacobians need many
-  // registers (capped for three blocks per SM), so small tiles keep every
-  // SM busy on meshes of a few thousand elements
+  // registers, so small tiles keep every SM busy on meshes of a few
+  // thousand elements
   static constexpr int TE = (8 * PER_ELE <= 64 * 1024) ? 8 : (4 * PER_ELE <= 64 * 1024) ? 4
                             : (2 * PER_ELE <= 64 * 1024) ? 2 : 1;
   static constexpr int NT = 128;
   static constexpr int SMEM = TE * PER_ELE;
 };
 
-// Element pass: one block per tile of TE elements.
+// Element pass: one block per tile of TE elements.  Registers are capped for
+// four blocks per SM on periodic meshes; the boundary variants, which also
+// carry the ghost states' Jacobians, spill about 2 KB a thread at that cap
+// (1.2 KB at three) and run faster capped for three.
 template <class C, bool BC, int RS>
-__global__ void __launch_bounds__(128, 3) fr_adj_elem_kernel(const AdjArgs a) {
+__global__ void __launch_bounds__(128, BC ? 3 : 4) fr_adj_elem_kernel(const AdjArgs a) {
   using T = AdjTile<C>;
   constexpr int TE = T::TE, NT = T::NT, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1;
   using D1 = ad::Dual<NV + 1>;  // own trace + the freestream parameter

@@ -667,7 +667,10 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       vm.fvn = s->vm.fvn;
       vm.fvn2 = s->vm.fvn2;
       const int nTiles = (s->nE + s->ks.vTE - 1) / s->ks.vTE;
-      s->ks.vgrad(&a, &vm, std::min(nTiles, s->nSM * s->ks.vgradOcc), s->ks.vgradSmem, s->stream);
+      // the gradient pass one tile per block (measured faster than its
+      // persistent form, which gains nothing from the L2 prefetch), the
+      // stage pass persistent
+      s->ks.vgrad(&a, &vm, nTiles, s->ks.vgradSmem, s->stream);
       if ((st = post_launch(s))) return st;
       s->ks.vstage(&a, &vm, std::min(nTiles, s->nSM * s->ks.vstageOcc), s->ks.vstageSmem, s->stream);
       st = post_launch(s);
