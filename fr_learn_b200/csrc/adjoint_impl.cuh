@@ -1,6 +1,8 @@
 // adjoint_impl.cuh -- launchers and the instantiation switch of the adjoint
 // kernels; included once per dimension unit after defining FRG_ADJ_DIM.
 #pragma once
+#include <array>
+
 #include "adjoint.cuh"
 #include "adjoint_visc.cuh"
 #include "dispatch.h"
@@ -58,6 +60,14 @@ void launch_adjv_elem(const AdjArgs &a, cudaStream_t st) {
   f.visc2 = a.v.visc2;
   f.dUg = a.v.g;
   f.ph = a.ph;
+  // this order's 1D operators for every VCJH scheme, built once
+  static const std::array<Ops1D, 4> ops = [] {
+    std::array<Ops1D, 4> t{};
+    for (int sch = 0; sch < 4; sch++)
+      if (!((sch == 3 && C::P < 2) || (sch == 2 && C::P == 0))) t[sch] = build_ops1d(C::P, sch);
+    return t;
+  }();
+  set_stage_ops(f, ops[a.vcjh]);
   fr_visc_grad_kernel<C, double, double, BC><<<(a.nEle + TV::TE - 1) / TV::TE, C::NT, TV::SMEM, st>>>(f);
   using T = AdjViscTile<C>;
   fr_adjv_elem_kernel<C, BC, RS><<<(a.nEle + T::TE - 1) / T::TE, T::NT, T::SMEM, st>>>(a);

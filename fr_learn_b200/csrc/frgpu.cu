@@ -425,6 +425,7 @@ StageArgs base_args(frg_solver *s) {
   a.ticket = s->ticket;
   a.cflFac = s->p.CFL * kCflLimit[s->p.order] * 2;
   a.nff = s->g.nFF;
+  set_stage_ops(a, s->ops);
   return a;
 }
 

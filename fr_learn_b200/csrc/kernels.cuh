@@ -207,7 +207,40 @@ struct StageArgs {
   double cflFac;
   int nff;
   Phys ph;
+  // the run's 1D operator tables (order, VCJH scheme), in the launch
+  // parameters so the kernels' unrolled loops read them as constant-bank
+  // operands rather than by indexed loads
+  OpTab<float> opf;
+  OpTab<double> opd;
 };
+
+template <typename R>
+__device__ __forceinline__ const OpTab<R> &stage_op(const StageArgs &a);
+template <>
+__device__ __forceinline__ const OpTab<double> &stage_op<double>(const StageArgs &a) { return a.opd; }
+template <>
+__device__ __forceinline__ const OpTab<float> &stage_op<float>(const StageArgs &a) { return a.opf; }
+// Host: fill a launch's tables from the 1D operators (setup.h Ops1D), cast
+// as the constant-memory copies are.
+template <class Ops>
+inline void set_stage_ops(StageArgs &a, const Ops &o) {
+  for (int i = 0; i <= KMAXP; i++) {
+    for (int h = 0; h < 2; h++) {
+      a.opd.lag[h][i] = o.lag[h][i];
+      a.opf.lag[h][i] = (float)o.lag[h][i];
+    }
+    a.opd.gL[i] = o.gL[i];
+    a.opd.gR[i] = o.gR[i];
+    a.opd.w[i] = o.w[i];
+    a.opf.gL[i] = (float)o.gL[i];
+    a.opf.gR[i] = (float)o.gR[i];
+    a.opf.w[i] = (float)o.w[i];
+    for (int j = 0; j <= KMAXP; j++) {
+      a.opd.dlag[i][j] = o.dlag[i][j];
+      a.opf.dlag[i][j] = (float)o.dlag[i][j];
+    }
+  }
+}
 
 // ----------------------------------------------------------------------------
 // The fused stage kernels and the block-level phases they share.
@@ -399,7 +432,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_kernel(const StageArgs a) {
   R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NSP][TE]
   R *Fs = Us + NV * NSP * TE;               // [DIM][NV][NSP][TE]
   R *Js = Fs + DIM * NV * NSP * TE;         // [NV][NF][TE]
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
   const Phys &ph = a.ph;
   const S *nrmG = static_cast<const S *>(a.nrm);
@@ -665,7 +698,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_visc_grad_kernel(const StageArgs 
   R *Us = reinterpret_cast<R *>(smem_raw);  // [NV][NSP][TE]
   R *Dc = Us + NV * NSP * TE;               // [NV][NF][TE]
   R *dUs = Dc + NV * NF * TE;               // [DIM][NV][NSP][TE]
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int e0 = blockIdx.x * TE;
   const S *nrmG = static_cast<const S *>(a.nrm);
   S *fvnOut = static_cast<S *>(a.fvnOut);
@@ -718,7 +751,7 @@ __global__ void __launch_bounds__(C::NT, 2) fr_stage_visc_kernel(const StageArgs
   R *Js = Us + NV * NSP * TE;               // [NV][NF][TE]: dUc, then the jumps
   R *dUs = Js + NV * NF * TE;               // [DIM][NV][NSP][TE]
   R *Fs = dUs + DIM * NV * NSP * TE;        // [DIM][NV][NSP][TE]
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int nE = a.nE, tid = threadIdx.x, e0 = blockIdx.x * TE;
   const Phys &ph = a.ph;
   const S *nrmG = static_cast<const S *>(a.nrm);

@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
   b.Wd = nullptr;  // wave speeds and dA read from global memory in phase B
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);
 
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x, e0 = blockIdx.x * TE;
   const int flags = a.flags;
   const bool last = flags & SF_LAST, jam = flags & SF_JAMESON;
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
   };
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);  // [NB][3]
 
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x;
   const int nTiles = (a.nEle + TE - 1) / TE;
   const int flags = a.flags;
@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);  // [2][3] ring groups, then U and Acc
   uint64_t *barU = bar + 6, *barA = bar + 7;
 
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x;
   const int nTiles = (a.nEle + TE - 1) / TE;
   const int flags = a.flags;

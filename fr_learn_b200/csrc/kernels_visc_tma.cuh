@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);
   S *FvO = reinterpret_cast<S *>(Dc);   // output after the gradient has read Dc
   S *Fv2 = reinterpret_cast<S *>(Ntr);  // penalty projection after the LDG phase has read Ntr
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x, nTiles = (a.nEle + TE - 1) / TE;
   const bool inU = a.Uin_d != nullptr;
   bool ok = true;
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   R *Js = Dc;                             // jumps, after the gradient has read Dc
   S *Wst = reinterpret_cast<S *>(JG);     // new stage state, after the fluxes have read JG
   S *TrO = reinterpret_cast<S *>(Ntr);    // new traces, after phase B has read Ntr
-  const OpTab<R> &op = optab<R>(a.vcjh, C::P);
+  const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x, flags = a.flags, nTiles = (a.nEle + TE - 1) / TE;
   const bool last = flags & SF_LAST, first = flags & SF_FIRST, jam = flags & SF_JAMESON;
   const TmaNeeds nd(a);
