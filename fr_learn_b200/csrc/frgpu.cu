@@ -1085,11 +1085,13 @@ frg_status frg_apply_operator(frg_solver *s, int which, int dim, const float *X,
   CUtensorMap mX;
   cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)K, (cuuint64_t)s->nV};
   cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)ld * 4 * K};
-  cuuint32_t box[3] = {128, (cuuint32_t)KP, 1};
+  // boxes of 32 elements (128 bytes) x KP points, 32-byte chunks swizzled
+  // within 128 bytes: the kernel's MN-major TF32 operand layout
+  cuuint32_t box[3] = {32, (cuuint32_t)KP, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(X), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(FRG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   CK(launch_op_gemm(mX, img, Y, KP, NP, M, ld, s->nE, s->nV, beta, s->err, s->stream));
   s->launches++;

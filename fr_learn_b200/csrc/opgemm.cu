@@ -12,24 +12,31 @@
 //   D[e][m] = sum_k A[e][k] B[k][m],   A = X_v^T (M = elements),
 //   B = Op^T (N = output points)
 //
-// with both operands K-major (8-row x 16-byte core matrices, no swizzle), so
-// the accumulator's TMEM lane is the element and its column the output
-// point: warp w reads lanes 32w..32w+31 and its 32 threads store 32
-// consecutive elements of each output point -- coalesced rows of Y.
+// A is read MN-major (elements contiguous) straight from the layout TMA lands
+// the tile in: four boxes of 32 elements x KP points, each row of 128 bytes
+// with its 32-byte chunks swizzled across 4-row groups -- the one MN-major
+// layout the TF32 MMA accepts, SWIZZLE_128B_BASE32B (4-row x 128-byte atoms;
+// 32-element groups LBO = KP * 128 bytes apart, 4-row groups 512 bytes apart),
+// which TMA writes with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.  (The plain
+// 128-byte swizzle, 16-byte chunks across 8 rows, is valid MN-major for
+// 16-bit operands; for TF32 the MMA produced zeros from it.)  B (the operator, prepared on
+// the host) is K-major without swizzle (8-row x 16-byte core matrices).  The
+// accumulator's TMEM lane is the element and its column the output point:
+// warp w reads lanes 32w..32w+31 and its 32 threads store 32 consecutive
+// elements of each output point -- coalesced rows of Y.
 //
 // Split precision: x = hi + lo with hi = tf32(x) (round to nearest) and
 // lo = tf32(x - hi); Op's halves are prepared on the host, X's by the block
-// after the tile lands, which also reorders the tile (points fastest) into
-// the K-major core matrices.  D = A_hi B_hi + A_lo B_hi + A_hi B_lo; the
-// dropped A_lo B_lo term and the rounding of the lo halves are ~2^-21
-// relative.
+// after the tile lands, elementwise and in place (hi over the landed tile, lo
+// at the same offsets of a second buffer): the swizzled positions need no
+// reordering.  D = A_hi B_hi + A_lo B_hi + A_hi B_lo; the dropped A_lo B_lo
+// term and the rounding of the lo halves are ~2^-21 relative.
 //
 // Persistent blocks over (128-element tile, field) pairs: one thread issues
-// the TMA loads (each tile as one [KP][128] box, the operator image once as
-// two bulk copies) on one mbarrier, the block splits and reorders the tile,
-// one thread issues this tile's MMAs (committed to a second mbarrier) and,
-// once they have read the tile, the next tile's load, and all four warps
-// drain TMEM.
+// the TMA loads (each tile as four [KP][32] boxes, the operator image once as
+// two bulk copies) on one mbarrier, the block splits the tile, one thread
+// issues this tile's MMAs (committed to a second mbarrier) and, once they
+// have read the tile, the next tile's loads, and all four warps drain TMEM.
 // Every wait is bounded; on expiry the block flags an error, lets its copies
 // and MMAs land (bounded again), frees its TMEM and returns.  No multicast.
 #include <cuda.h>
@@ -54,18 +61,21 @@ __device__ __forceinline__ float tf32_rna(float x) {
 }
 
 // Shared-memory matrix descriptor (tcgen05 matrix descriptor): start,
-// leading and stride byte offsets in 16-byte units, version 1 in bits 46-48,
-// layout type 0 (no swizzle) in bits 61-63.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// leading and stride byte offsets in 16-byte units (bits 0-13, 16-29,
+// 32-45), version 1 in bits 46-47, base offset 0, layout type in bits 61-63
+// (0: no swizzle, 1: 128-byte swizzle of 32-byte chunks).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout = 0) {
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
 }
+constexpr uint32_t kLayoutSW128Base32 = 1;
 
 // Instruction descriptor of kind::tf32: F32 accumulator (bits 4-5), TF32 A
-// and B (bits 7-9, 10-12), both K-major (bits 15, 16 clear), N >> 3 in bits
-// 17-22, M >> 4 in bits 24-28 with M = 128.
+// and B (bits 7-9, 10-12), A MN-major (bit 15), B K-major (bit 16 clear),
+// N >> 3 in bits 17-22, M >> 4 in bits 24-28 with M = 128.
 __host__ __device__ constexpr uint32_t idesc_tf32(int n) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
 }
 
 __device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t accum) {
@@ -102,23 +112,24 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 // Y_v = Op X_v (+ beta Y_v) over tiles of 128 elements of one field; tile t
 // covers elements [128 (t % nT), +128) of field t / nT, nT = ceil(nEle/128).
 // Persistent: block b takes tiles b, b + gridDim.x, ...; the operator image
-// is loaded once, and the next tile's TMA load is issued as soon as the
-// current tile's MMAs have read it, so it lands while the accumulator is
-// drained (and while the SM's other block computes).  KP: K padded to a multiple of 8; NP: output points padded to a
-// multiple of 16; M: real output points; ncol: TMEM columns allocated (a
-// power of two >= NP).  Bimg: the operator image (see build_op_image).
-// Shared memory: the landed tile [KP][128] (rewritten in place as A_hi),
-// A_lo, both as K-major core matrices [KP/8][16][2][8][4], the image, two
-// mbarriers, the TMEM address: 112 KB for a 64 x 96 operator, two blocks
-// per SM.
+// is loaded once, and the next tile's TMA loads are issued as soon as the
+// current tile's MMAs have read it, so they land while the accumulator is
+// drained (and while the SM's other block computes).  KP: K padded to a
+// multiple of 8; NP: output points padded to a multiple of 16; M: real output
+// points; ncol: TMEM columns allocated (a power of two >= NP).  Bimg: the
+// operator image (see build_op_image).  mX: 3D map [field][K][ld] with box
+// {32, KP, 1} and the 128-byte swizzle of 32-byte chunks.  Shared memory (1024-byte aligned):
+// the landed tile (4 x [KP][32], rewritten in place as A_hi), A_lo at the same
+// offsets, the image, two mbarriers, the TMEM address: 112 KB for a 64 x 96
+// operator, two blocks per SM.
 __global__ void __launch_bounds__(128, 1)
     fr_op_gemm_tc_kernel(const __grid_constant__ CUtensorMap mX, const float *__restrict__ Bimg, float *Y, int KP,
                          int NP, int M, int ncol, int ld, int nEle, int nV, float beta, unsigned *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char *const sb = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  unsigned char *const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
+  const uint32_t boxBytes = (uint32_t)KP * 128u;  // one [KP][32] box: the stride between 32-element groups
   float *St = reinterpret_cast<float *>(sb);  // the landed tile, turned into A_hi in place
-  float *Ahi = St;
   float *Alo = reinterpret_cast<float *>(sb + aBytes);
   float *Bs = reinterpret_cast<float *>(sb + 2 * aBytes);  // hi, then lo
   const uint32_t bHalf = (uint32_t)KP * NP * 4u;
@@ -144,10 +155,15 @@ __global__ void __launch_bounds__(128, 1)
   tc_fence_after();
   const uint32_t tmem = *tslot;
 
+  // thread 0: tile t's four 32-element boxes into St
+  auto load_tile = [&](int t) {
+    for (int q = 0; q < 4; q++)
+      tma_load3d(reinterpret_cast<unsigned char *>(St) + q * boxBytes, &mX, (t % nT) * 128 + 32 * q, 0, t / nT,
+                 &bar[0]);
+  };
   if (tid == 0) {
-    const int t = blockIdx.x;
     mbar_expect_tx(&bar[0], aBytes + 2u * bHalf);
-    tma_load3d(St, &mX, (t % nT) * 128, 0, t / nT, &bar[0]);
+    load_tile(blockIdx.x);
     bulk_load(Bs, Bimg, bHalf, &bar[0]);
     bulk_load(reinterpret_cast<unsigned char *>(Bs) + bHalf, reinterpret_cast<const unsigned char *>(Bimg) + bHalf,
               bHalf, &bar[0]);
@@ -161,48 +177,39 @@ __global__ void __launch_bounds__(128, 1)
     ok = mbar_wait(&bar[0], par);
     if (__syncthreads_or(!ok)) break;
     loadsDone++;
-    // split and reorder: thread = element e; each group of four consecutive
-    // points becomes one 16-byte row of a core matrix (K step s = k/8, half
-    // h = (k%8)/4, row group g = e/8, row r = e%8).  The core matrices of K
-    // step s occupy exactly the bytes of landed rows 8s..8s+7, so A_hi is
-    // written in place, one 8-row block at a time: every thread reads its
-    // column of the block, the block synchronises, then the block is
-    // rewritten.  The previous tile's MMAs have completed (waited below).
+    // split, elementwise: the swizzle moves whole 32-byte chunks, so hi and
+    // lo keep the landed positions (the previous tile's MMAs have completed,
+    // waited below)
     {
-      const int e = tid, g = e >> 3, r = e & 7;
-      for (int sk = 0; sk < KP / 8; sk++) {
-        float x[8];
-#pragma unroll
-        for (int c = 0; c < 8; c++) x[c] = St[(8 * sk + c) * 128 + e];
-        __syncthreads();
-#pragma unroll
-        for (int hh = 0; hh < 2; hh++) {
-          float4 h, l;
-          h.x = tf32_rna(x[4 * hh + 0]);
-          h.y = tf32_rna(x[4 * hh + 1]);
-          h.z = tf32_rna(x[4 * hh + 2]);
-          h.w = tf32_rna(x[4 * hh + 3]);
-          l.x = tf32_rna(x[4 * hh + 0] - h.x);
-          l.y = tf32_rna(x[4 * hh + 1] - h.y);
-          l.z = tf32_rna(x[4 * hh + 2] - h.z);
-          l.w = tf32_rna(x[4 * hh + 3] - h.w);
-          const int o = sk * 1024 + g * 64 + hh * 32 + r * 4;
-          *reinterpret_cast<float4 *>(Ahi + o) = h;
-          *reinterpret_cast<float4 *>(Alo + o) = l;
-        }
+      float4 *S4 = reinterpret_cast<float4 *>(St), *L4 = reinterpret_cast<float4 *>(Alo);
+      for (int i = tid; i < KP * 32; i += 128) {
+        const float4 x = S4[i];
+        float4 h, l;
+        h.x = tf32_rna(x.x);
+        h.y = tf32_rna(x.y);
+        h.z = tf32_rna(x.z);
+        h.w = tf32_rna(x.w);
+        l.x = tf32_rna(x.x - h.x);
+        l.y = tf32_rna(x.y - h.y);
+        l.z = tf32_rna(x.z - h.z);
+        l.w = tf32_rna(x.w - h.w);
+        S4[i] = h;
+        L4[i] = l;
       }
     }
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t aHi = smem_u32(Ahi), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
-      // core matrices: the two K halves 128 bytes apart (leading offset),
-      // 8-row groups 256 bytes apart (stride offset); one K step of 8 spans
-      // 16 groups of A (4096 bytes) and NP/8 groups of B (NP*32 bytes)
+      const uint32_t aHi = smem_u32(St), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
+      // A (MN-major, 32-byte-chunk swizzle): K step s is rows 8s..8s+7,
+      // two 512-byte atoms of 4 rows, in every box; the boxes boxBytes apart
+      // (leading offset), 4-row groups 512 bytes apart (stride offset).  B (K-major,
+      // no swizzle): the two K halves 128 bytes apart (leading offset),
+      // 8-row groups 256 bytes apart (stride offset), NP/8 groups per K step
       for (int s = 0; s < KP / 8; s++) {
-        const uint64_t ah = smem_desc(aHi + s * 4096, 128, 256);
-        const uint64_t al = smem_desc(aLo + s * 4096, 128, 256);
+        const uint64_t ah = smem_desc(aHi + s * 1024, boxBytes, 512, kLayoutSW128Base32);
+        const uint64_t al = smem_desc(aLo + s * 1024, boxBytes, 512, kLayoutSW128Base32);
         const uint64_t bh = smem_desc(bHi + s * NP * 32, 128, 256);
         const uint64_t bl = smem_desc(bLo + s * NP * 32, 128, 256);
         tc_mma(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
@@ -221,7 +228,7 @@ __global__ void __launch_bounds__(128, 1)
       const int tn = t + gridDim.x;
       if (tn < nTiles) {
         mbar_expect_tx(&bar[0], aBytes);
-        tma_load3d(St, &mX, (tn % nT) * 128, 0, tn / nT, &bar[0]);
+        load_tile(tn);
         loads++;
       }
     }
@@ -303,7 +310,7 @@ void build_op_image(const double *op, int M, int K, int KP, int NP, std::vector<
           }
 }
 
-size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 2 + (size_t)2 * KP * NP * 4 + 64 + 128; }
+size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 2 + (size_t)2 * KP * NP * 4 + 64 + 1024; }
 
 cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
                            int nEle, int nV, float beta, unsigned *err, cudaStream_t st) {
