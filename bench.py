@@ -485,8 +485,11 @@ def run_ensemble(stream, nsteps=500, warmup=3, alone_steps=20, adj_steps=100):
         s.set_stream(None)
         s.close()
 
-    # adjoint of the per-case entropy error, FP64, per order group
-    fwd_ms = adj_ms = 0.0
+    # adjoint of the per-case entropy error, FP64, per order group: with the
+    # automatic memory strategy (every stage state kept when that fits in half
+    # of the free memory) and with checkpoints every 25 steps (recomputation
+    # overlapped with the reversal)
+    fwd_ms, adj_ms, kept = 0.0, {"auto": 0.0, "checkpoint_25": 0.0}, {}
     for P, _, union, grp, U in solvers:
         a = Solver(union, order=P, dtType=0, dt=1.0, precision=FRG_FP64, **kw)
         a.set_groups(grp, grp.max() + 1, first_dt[P])
@@ -496,18 +499,22 @@ def run_ensemble(stream, nsteps=500, warmup=3, alone_steps=20, adj_steps=100):
             a.update(1)
         a.set("U_spts", U)
         fwd_ms += timed(lambda: a.update(adj_steps))
-        # one untimed forward + reverse sweep first: the segment graphs and the
-        # stage slots are made on first use (set-up, like the forward's warm-up)
-        for timed_run in (False, True):
-            a.set("U_spts", U)
-            with torch.cuda.stream(stream):
-                a.adjoint_forward(adj_steps, 25)
-                a.objective("entropy")
-            if timed_run:
-                adj_ms += timed(lambda: a.adjoint_backward())
-            else:
+        for mode, every in (("checkpoint_25", 25), ("auto", -1)):
+            # one untimed forward + reverse sweep first: the segment graphs and
+            # the stage slots are made on first use (set-up, like the forward's
+            # warm-up)
+            for timed_run in (False, True):
+                a.set("U_spts", U)
                 with torch.cuda.stream(stream):
-                    a.adjoint_backward()
+                    a.adjoint_forward(adj_steps, every)
+                    a.objective("entropy")
+                if timed_run:
+                    adj_ms[mode] += timed(lambda: a.adjoint_backward())
+                else:
+                    with torch.cuda.stream(stream):
+                        a.adjoint_backward()
+            if mode == "auto":
+                kept[str(P)] = a.adjoint_mode()
         a.set_stream(None)
         a.close()
     return {"workload": "256 isentropic-vortex cases, side {16..96}, P {2..5}, strength U[1,5], Mach U[0.1,0.6], "
@@ -517,8 +524,14 @@ def run_ensemble(stream, nsteps=500, warmup=3, alone_steps=20, adj_steps=100):
             "ensemble_value": ens_rate, "ensemble_ms_per_step": ms / nsteps, "unit": "DOF-updates/s",
             "one_by_one_value": alone_rate, "one_by_one_steps_per_case": alone_steps,
             "ensemble_over_one_by_one": ens_rate / alone_rate,
-            "adjoint_fp64": {"steps": adj_steps, "checkpoint_every": 25, "forward_ms_per_step": fwd_ms / adj_steps,
-                             "adjoint_ms_per_step": adj_ms / adj_steps, "adjoint_over_forward": adj_ms / fwd_ms,
+            "adjoint_fp64": {"steps": adj_steps, "forward_ms_per_step": fwd_ms / adj_steps,
+                             "adjoint_ms_per_step": adj_ms["auto"] / adj_steps,
+                             "adjoint_over_forward": adj_ms["auto"] / fwd_ms,
+                             "checkpoint_every_per_order": kept,
+                             "memory": "auto: every stage state kept when it fits in half of the free device memory "
+                                       "(0 = all kept), else checkpoints every 25 steps",
+                             "checkpoint_every_25": {"adjoint_ms_per_step": adj_ms["checkpoint_25"] / adj_steps,
+                                                     "adjoint_over_forward": adj_ms["checkpoint_25"] / fwd_ms},
                              "objective": "per-case entropy error integral at the final time"}}
 
 

@@ -142,7 +142,8 @@ template <class C, bool BC, int RS>
 __global__ void __launch_bounds__(128, BC ? 3 : 4) fr_adj_elem_kernel(const AdjArgs a) {
   using T = AdjTile<C>;
   constexpr int TE = T::TE, NT = T::NT, NS = C::NS, NF = C::NF, NV = C::NV, DIM = C::DIM, N1 = C::N1;
-  using D1 = ad::Dual<NV + 1>;  // own trace + the freestream parameter
+  // own trace, and with boundaries the freestream parameter the ghost states take
+  using D1 = ad::Dual<BC ? NV + 1 : NV>;
   using D0 = ad::Dual<NV>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sY = reinterpret_cast<double *>(smem_raw);

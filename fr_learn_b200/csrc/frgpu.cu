@@ -2165,11 +2165,21 @@ frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double
 }
 
 frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery) {
-  if (!s || nsteps < 1 || checkpointEvery < 0) return fail(FRG_ERR_ARG, "bad arguments");
+  if (!s || nsteps < 1) return fail(FRG_ERR_ARG, "bad arguments");
   frg_status st;
   if ((st = adj_check_path(s)) || (st = adj_init(s))) return st;
   AdjState *a = s->adj;
   const size_t nSE = (size_t)s->nV * s->nS * s->L;
+  if (checkpointEvery < 0) {
+    // keep every stage state when they fit in half of the free memory (the
+    // stage slots a previous run holds count as free)
+    size_t freeB = 0, totalB = 0;
+    CK(cudaMemGetInfo(&freeB, &totalB));
+    const size_t held = (a->stages ? nSE * (size_t)a->stagesCap * s->nRK * 8 : 0) +
+                        (a->stages2 ? nSE * (size_t)a->stagesCap * s->nRK * 8 : 0);
+    const size_t need = nSE * (size_t)nsteps * s->nRK * 8;
+    checkpointEvery = need <= (freeB + held) / 2 ? 0 : 25;
+  }
   // checkpointEvery 0: keep every stage state of the run (no recomputation)
   const bool keepAll = checkpointEvery == 0;
   const int k = keepAll ? nsteps : std::min(checkpointEvery, nsteps);
@@ -2219,6 +2229,13 @@ frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery) {
   CK(cudaMemcpyAsync(a->ckpt + nSE * nCkpt, s->U, nSE * 8, cudaMemcpyDeviceToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return check_flags(s);
+}
+
+frg_status frg_adjoint_mode(const frg_solver *s, int *checkpointEvery) {
+  if (!s || !checkpointEvery) return fail(FRG_ERR_ARG, "null argument");
+  if (!s->adj || s->adj->nSteps < 1) return fail(FRG_ERR_ARG, "adjoint: no recorded forward run (frg_adjoint_forward)");
+  *checkpointEvery = s->adj->keepAll ? 0 : s->adj->k;
+  return FRG_OK;
 }
 
 frg_status frg_adjoint_backward(frg_solver *s, const double *lamN_host, const double *thetaDir, double *lam0_host,

@@ -329,8 +329,12 @@ __device__ __forceinline__ void tma_phase_b(const StageArgs &a, const OpTab<R> &
 // element-fastest, then line, then field, so the lane groups of a warp
 // fall on different shared-memory banks (the field stride of the flux-point
 // arrays is a multiple of 32 words).  Contains a block barrier between the
-// passes.
-template <class C, typename R, typename S, int TE, int NT>
+// passes.  The RK update scales the divergence by 1/detJ in the arithmetic
+// type, then by the stage's coefficient x dt in FP64.  COLTR: pass C2, which
+// holds each column of the new state, also writes the column's bottom and
+// top traces into TrO (phase D then does the rows): the sums phase D would
+// form, in the same order over the same values.
+template <class C, typename R, typename S, int TE, int NT, bool COLTR = false>
 __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &op, const TmaBufs<R, S> &b, int e0,
                                             double dtG) {
   constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1;
@@ -359,10 +363,12 @@ __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &
     const int e = it % TE, r = it / TE, i = r % N1, v = r / N1, eg = e0 + e;
     if (eg >= a.nEle) continue;
     const double dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
+    const double cb = a.bCur * dtl, ca = a.aNext * dtl;
     R F[N1];
 #pragma unroll
     for (int q = 0; q < N1; q++) F[q] = b.Fs[((1 * NV + v) * NS + q * N1 + i) * TE + e];
     const R JB = b.Js[(v * NF + i) * TE + e], JT = b.Js[(v * NF + 2 * N1 + C::P - i) * TE + e];
+    R t0 = 0, t1 = 0;  // COLTR: the column's bottom / top traces
 #pragma unroll
     for (int j = 0; j < N1; j++) {
       const int s = j * N1 + i, o = (v * NS + s) * TE + e;
@@ -371,15 +377,14 @@ __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &
       for (int q = 0; q < N1; q++) acc += op.dlag[j][q] * F[q];
       acc += -op.gL[j] * JB;
       acc += op.gR[j] * JT;
-      const double idet = (double)b.Det[s * TE + e];  // 1 / detJ
-      const double div = (double)acc;
-      if (flags & SF_DIVF) a.divF[((size_t)v * NS + s) * a.ldU + eg] = div;
+      if (flags & SF_DIVF) a.divF[((size_t)v * NS + s) * a.ldU + eg] = (double)acc;
+      const double dj = (double)(acc * (R)b.Det[s * TE + e]);  // divF / detJ
       double unew;
       if (jam) {
-        unew = b.U0[o] - a.aNext * div * idet * dtl;
+        unew = b.U0[o] - ca * dj;
         if (last) b.U0[o] = unew;
       } else {
-        const double t = a.bCur * div * idet * dtl;
+        const double t = cb * dj;
         const double base = first ? b.U0[o] : b.Acc[o];
         if (last) {
           unew = base - t;
@@ -387,23 +392,33 @@ __device__ __forceinline__ void tma_phase_c(const StageArgs &a, const OpTab<R> &
         } else {
           b.Acc[o] = base - t;
           const double u0 = first ? base : b.U0[o];
-          unew = u0 - a.aNext * div * idet * dtl;
+          unew = u0 - ca * dj;
         }
       }
       if (last && (v == 0 || v == NV - 1) && isnan(unew)) atomicOr(a.err, ERRF_NAN);
-      b.Us[o] = (R)(last ? unew : (double)(S)unew);
+      const R un = (R)(last ? unew : (double)(S)unew);
+      b.Us[o] = un;
+      if (COLTR) {
+        t0 += op.lag[0][j] * un;
+        t1 += op.lag[1][j] * un;
+      }
+    }
+    if (COLTR) {
+      b.TrO[(v * NF + i) * TE + e] = (S)t0;
+      b.TrO[(v * NF + 2 * N1 + C::P - i) * TE + e] = (S)t1;
     }
   }
 }
 
 // Phase D: traces of the new state into TrO; one item per (line, field,
 // element) gives the traces at both ends of the line (rows: left face 3 /
-// right face 1; columns: bottom face 0 / top face 2).
-template <class C, typename R, typename S, int TE, int NT>
+// right face 1; columns: bottom face 0 / top face 2).  ROWS: the rows only
+// (phase C wrote the columns').
+template <class C, typename R, typename S, int TE, int NT, bool ROWS = false>
 __device__ __forceinline__ void tma_phase_d(const OpTab<R> &op, const R *Us, S *TrO) {
-  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1;
-  for (int it = threadIdx.x; it < 2 * N1 * NV * TE; it += NT) {
-    const int e = it % TE, r = it / TE, ln = r % (2 * N1), v = r / (2 * N1);
+  constexpr int NS = C::NS, NF = C::NF, NV = C::NV, N1 = C::N1, NL = ROWS ? N1 : 2 * N1;
+  for (int it = threadIdx.x; it < NL * NV * TE; it += NT) {
+    const int e = it % TE, r = it / TE, ln = r % NL, v = r / NL;
     const bool row = ln < N1;
     const int k = row ? ln : ln - N1;
     const int s0 = row ? k * N1 : k, st = row ? 1 : N1;
@@ -703,7 +718,7 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
     tma_phase_b<C, R, S, BC, RS, TE, NT>(a, op, b, e0);
     ok = mbar_wait(&bk[2], par);
     if (__syncthreads_or(!ok)) break;
-    tma_phase_c<C, R, S, TE, NT>(a, op, b, e0, dtG);
+    tma_phase_c<C, R, S, TE, NT, true>(a, op, b, e0, dtG);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
@@ -714,7 +729,7 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
       }
       tma_commit();
     }
-    tma_phase_d<C, R, S, TE, NT>(op, b.Us, b.TrO);
+    tma_phase_d<C, R, S, TE, NT, true>(op, b.Us, b.TrO);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
@@ -957,7 +972,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
       aDone += ok;
     }
     if (__syncthreads_or(!ok)) break;
-    tma_phase_c<C, R, S, TE, NT>(a, op, b, e0, dtG);
+    tma_phase_c<C, R, S, TE, NT, true>(a, op, b, e0, dtG);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
@@ -975,7 +990,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
         uIss++;
       }
     }
-    tma_phase_d<C, R, S, TE, NT>(op, b.Us, b.TrO);
+    tma_phase_d<C, R, S, TE, NT, true>(op, b.Us, b.TrO);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {

@@ -652,8 +652,9 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
     const int ijk[3] = {i, j, k};
     int cf[2 * DIM], cs[2 * DIM], ca[2 * DIM];
     corr_fpts<C>(i, j, k, cf, cs, ca);
-    const double idet = (double)Det[s * TE + e];  // 1 / detJ
+    const R idet = (R)Det[s * TE + e];  // 1 / detJ
     const double dtl = a.grp ? a.dt[a.grp[eg]] : a.dtLocal ? a.dt[eg] : dtG;
+    const double kb = a.bCur * dtl, ka = a.aNext * dtl;
 #pragma unroll
     for (int v = 0; v < NV; v++) {
       R acc = 0;
@@ -671,15 +672,16 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
         acc += gcf * Js[(v * NF + cf[c]) * TE + e];
       }
       const int o = (v * NS + s) * TE + e;
-      const double div = (double)acc;
-      if (flags & SF_DIVF) a.divF[((size_t)v * NS + s) * a.ldU + eg] = div;
+      if (flags & SF_DIVF) a.divF[((size_t)v * NS + s) * a.ldU + eg] = (double)acc;
+      // divF / detJ in the arithmetic type, the stage coefficient x dt in FP64
+      const double dj = (double)(acc * idet);
       double unew;
       if (jam) {
-        unew = U0[o] - a.aNext * div * idet * dtl;
+        unew = U0[o] - ka * dj;
         if (last) U0[o] = unew;
         else Wst[o] = (S)unew;
       } else {
-        const double t = a.bCur * div * idet * dtl;
+        const double t = kb * dj;
         const double base = first ? U0[o] : Acc[o];
         if (last) {
           unew = base - t;
@@ -687,7 +689,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
         } else {
           Acc[o] = base - t;
           const double u0 = first ? base : U0[o];
-          unew = u0 - a.aNext * div * idet * dtl;
+          unew = u0 - ka * dj;
           Wst[o] = (S)unew;
         }
       }

@@ -116,6 +116,7 @@ def lib():
         "frg_get_group_times": ([vp, vp, vp], i),
         "frg_residual_vjp": ([vp, vp, vp, vp, C.POINTER(d)], i),
         "frg_adjoint_forward": ([vp, i, i], i),
+        "frg_adjoint_mode": ([vp, C.POINTER(i)], i),
         "frg_adjoint_backward": ([vp, vp, vp, vp, C.POINTER(d)], i),
         "frg_read_gmsh": ([C.c_char_p, C.c_char_p, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp, vp, vp], i),
         "frg_wall_force": ([vp, vp], i),
@@ -389,8 +390,16 @@ class Solver:
         return out, tb.value
 
     def adjoint_forward(self, nsteps, checkpoint_every=25):
-        """nsteps of update() keeping checkpoints for adjoint_backward()."""
+        """nsteps of update() keeping checkpoints for adjoint_backward()
+        (checkpoint_every 0: every stage state kept; -1: every stage state
+        kept if it fits in half of the free device memory, else 25)."""
         _check(lib().frg_adjoint_forward(self.h, nsteps, checkpoint_every))
+
+    def adjoint_mode(self):
+        """The last adjoint_forward run's checkpoint interval (0: all kept)."""
+        k = C.c_int(0)
+        _check(lib().frg_adjoint_mode(self.h, C.byref(k)))
+        return k.value
 
     def adjoint_backward(self, lamN=None, theta_dir=None):
         """(dJ/dU_0, dJ/dtheta through the boundary state) for the last

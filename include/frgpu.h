@@ -349,10 +349,18 @@ frg_status frg_residual_vjp(frg_solver *s, const double *gbar_host, const double
 
 /* Forward run of nsteps frg_update steps keeping a checkpoint of U every
  * checkpointEvery steps (device memory: nsteps/checkpointEvery + 2 states,
- * plus checkpointEvery x nRK stage states for the reverse sweep).
- * checkpointEvery 0 keeps every RK stage state of the run instead
- * (nsteps x nRK states), so the reverse sweep recomputes nothing. */
+ * plus checkpointEvery x nRK stage states for the reverse sweep, twice when
+ * the recomputation overlaps the reversal).  checkpointEvery 0 keeps every
+ * RK stage state of the run instead (nsteps x nRK states), so the reverse
+ * sweep recomputes nothing.  checkpointEvery < 0 (FRG_CHECKPOINT_AUTO) keeps
+ * every stage state when they take at most half of the device memory free
+ * at the call, else checkpoints every 25 steps; frg_adjoint_mode reports the
+ * choice. */
+#define FRG_CHECKPOINT_AUTO (-1)
 frg_status frg_adjoint_forward(frg_solver *s, int nsteps, int checkpointEvery);
+/* The last frg_adjoint_forward run's checkpoint interval (0: every stage
+ * state kept). */
+frg_status frg_adjoint_mode(const frg_solver *s, int *checkpointEvery);
 /* Reverse sweep of the last frg_adjoint_forward run: from lamN = dJ/dU_N
  * ([spt][ele][field]; NULL = the gradient of the last frg_objective call)
  * to lam0 = dJ/dU_0 and thetaBar = dJ/dtheta through the boundary state
