@@ -228,22 +228,26 @@ def test_autograd_binding_matches_central_differences():
 
 
 def test_checkpointed_and_stored_sweeps_agree():
-    """Checkpoint intervals 1, 3 and 'keep everything' give the same dJ/dU_0."""
+    """Checkpoint intervals 1, 3, 'keep everything' and the automatic choice
+    give the same dJ/dU_0."""
     from fr_learn_b200 import bump2d
 
     c = np.sqrt(GAMMA)
     mesh = bump2d(6, 3, bc_top="symmetry")
     kw = dict(order=3, riemannType=1, uBound=0.5 * c, pBound=1.0)
     out = []
-    for every in (1, 3, 0):
+    for every in (1, 3, 0, -1):
         s = _solver(mesh, 0, **kw)
         s.adjoint_forward(8, every)
+        # the automatic strategy keeps every stage state of a run this small
+        assert s.adjoint_mode() == (0 if every <= 0 else every)
         s.objective("wall_pressure")
         out.append(s.adjoint_backward(None, np.array([0.0, c, 0, 0, 0]))[0])
         # a second sweep replays the captured segment graphs (both slot sets of
         # the overlapped recompute / reverse) and must give the same bits
         assert np.array_equal(s.adjoint_backward(None, np.array([0.0, c, 0, 0, 0]))[0], out[-1])
     assert relerr(out[1], out[0]) < 1e-12 and relerr(out[2], out[0]) < 1e-12
+    assert np.array_equal(out[3], out[2])
 
 
 # ---- viscous (LDG) residuals: the three-pass viscous adjoint
