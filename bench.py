@@ -223,6 +223,9 @@ def run_gpu(args, rank, world, local_rank):
                 ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                       for _ in range(args.steps)]
                 sampler.mark(True)
+                # an NVTX range names the timed region (profiler launch lists:
+                # ncu --nvtx --nvtx-include "timed_<precision>/")
+                torch.cuda.nvtx.range_push(f"timed_{name}")
                 t_wall = time.perf_counter()
                 for k in range(args.steps):
                     flush.fill_(k & 0xFF)
@@ -231,6 +234,7 @@ def run_gpu(args, rank, world, local_rank):
                     ev[k][1].record(stream)
                 stream.synchronize()
                 t_wall = time.perf_counter() - t_wall
+                torch.cuda.nvtx.range_pop()
                 sampler.mark(False)
                 if world > 1:
                     torch.distributed.barrier()

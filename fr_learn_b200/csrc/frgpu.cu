@@ -711,6 +711,7 @@ frg_status check_flags(frg_solver *s) {
     if (h & ERRF_DT) return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
     if (h & ERRF_NAN) return fail(FRG_ERR_NAN, "NaN encountered in the solution");
     if (h & ERRF_BC) return fail(FRG_ERR_ARG, "Boundary condition not recognized");
+    if (h & ERRF_ALIGN) return fail(FRG_ERR_CUDA, "operator GEMM: dynamic shared memory not 1024-byte aligned");
     if (h & ERRF_TIMEOUT) return fail(FRG_ERR_TIMEOUT, "a bounded device wait gave up");
   }
   return FRG_OK;

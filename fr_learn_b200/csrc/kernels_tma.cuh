@@ -24,7 +24,7 @@
 
 namespace frg {
 
-enum : unsigned { ERRF_TIMEOUT = 8u };
+enum : unsigned { ERRF_TIMEOUT = 8u, ERRF_ALIGN = 16u };
 
 // Tensor maps of one stage launch (all 2D: [rows][element stride]).
 struct TmaMaps {
@@ -908,9 +908,11 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     uint64_t *bk = &bar[3 * k];
     const int e0 = t * TE;
     if (tid == 0) {
-      // the previous tile's stores have been read out before the FP64
-      // buffers and the other slot are reused
-      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      // the previous tile's state / accumulator stores have been read out
+      // before the FP64 buffers and the other slot are reused; its trace
+      // store (the most recent group) reads only that slot's trace buffer,
+      // next written by the tile after this one, after its own wait
+      asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
       if (nd.needAcc) {
         issue_acc(b, e0);
         aIss++;
@@ -932,13 +934,13 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     // second round leaves idle; Ws is rewritten only in this tile's phase B
     if (dtn && prevE0 >= 0 && (tid >> 5) == NT / 32 - 1)
       dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, prevE0, tid & 31));
-    if (tid == 0) {
+    // the next tile's loads, issued by the last thread, which has one phase-A
+    // item where thread 0 has two (thread 0 keeps the counts)
+    if (tid == NT - 1) {
       const int tn = t + gridDim.x;
-      if (tn < nTiles) {
-        issue_slot(slot(k ^ 1), tn * TE, &bar[3 * (k ^ 1)], 0);
-        sIss++;
-      }
+      if (tn < nTiles) issue_slot(slot(k ^ 1), tn * TE, &bar[3 * (k ^ 1)], 0);
     }
+    if (tid == 0 && t + gridDim.x < nTiles) sIss++;
     if (dtn) {
       // the next tile's stored wave speeds and dA into L2, so its gathers
       // (at its start) do not wait on DRAM

@@ -125,8 +125,14 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 __global__ void __launch_bounds__(128, 1)
     fr_op_gemm_tc_kernel(const __grid_constant__ CUtensorMap mX, const float *__restrict__ Bimg, float *Y, int KP,
                          int NP, int M, int ncol, int ld, int nEle, int nV, float beta, unsigned *err) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char *const sb = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  // the swizzled tiles need 1024-byte alignment; the dynamic shared memory
+  // starts there (checked: no slack is allocated, so that two blocks fit)
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *const sb = smem_raw;
+  if (smem_u32(smem_raw) & 1023u) {
+    if (threadIdx.x == 0) atomicOr(err, ERRF_ALIGN);
+    return;
+  }
   const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
   const uint32_t boxBytes = (uint32_t)KP * 128u;  // one [KP][32] box: the stride between 32-element groups
   float *St = reinterpret_cast<float *>(sb);  // the landed tile, turned into A_hi in place
@@ -310,7 +316,7 @@ void build_op_image(const double *op, int M, int K, int KP, int NP, std::vector<
           }
 }
 
-size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 2 + (size_t)2 * KP * NP * 4 + 64 + 1024; }
+size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 2 + (size_t)2 * KP * NP * 4 + 64; }
 
 cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
                            int nEle, int nV, float beta, unsigned *err, cudaStream_t st) {
