@@ -623,13 +623,16 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
   if (s->p.dtType != 0) {
     if (mode == 2 && (st = launch_wavesp(s))) return st;
     if (mode >= 1 && (st = launch_dt(s))) return st;
-    if (fused_dt(s) && !s->grp)  // the slot the last stage will minimise into
+    // the slot the last stage will minimise into: reset by the first stage
+    // (a memset only when one stage is also the last)
+    if (fused_dt(s) && !s->grp && s->nRK == 1)
       CK(cudaMemsetAsync(s->dtDev + (s->dtCur ^ 1), 0x7F, sizeof(double), s->stream));
   }
   if (s->grp && (st = launch_group_step(s))) return st;
   if (ev) CK(cudaEventRecord(ev[1], s->stream));
   const int nRK = s->nRK;
   const bool jam = s->p.timeType == 5;
+  double *const dtReset = (fused_dt(s) && !s->grp && nRK > 1) ? s->dtDev + (s->dtCur ^ 1) : nullptr;
   for (int k = 0; k < nRK; k++) {
     StageArgs a = base_args(s);
     const bool first = k == 0, last = k == nRK - 1;
@@ -650,6 +653,7 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       a.divF = s->divF[0];
     }
     if (last && fused_dt(s)) a.flags |= SF_DTNEXT;
+    if (first) a.dtReset = dtReset;
     // stages after the first follow a stage kernel directly: programmatic
     // dependent launch (not when each launch is timed on its own)
     if (k > 0 && s->pdl && !ev) a.flags |= SF_PDL;

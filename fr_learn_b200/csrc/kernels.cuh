@@ -203,6 +203,9 @@ struct StageArgs {
   // SF_DTNEXT: the next step's dt (ele::calcDt + the global minimum)
   const double *vol, *dAd, *wsurf;
   double *blockMin, *dtNext, *eleDt;
+  // first stage of a step with the fused dt (TMA kernels): the next step's dt
+  // slot, set here to a huge value before the last stage minimises into it
+  double *dtReset;
   unsigned *ticket;
   double cflFac;
   int nff;

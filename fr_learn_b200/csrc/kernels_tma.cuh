@@ -101,6 +101,13 @@ __device__ __forceinline__ void pdl_launch_dependents() {
 }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// First stage of a step with the fused dt: the slot the last stage will
+// minimise the next dt into starts at a huge value (the bytes 0x7F, as a
+// memset before the step would leave it); the stages in between do not read it.
+__device__ __forceinline__ void stage_dt_reset(const StageArgs &a) {
+  if (a.dtReset && blockIdx.x == 0 && threadIdx.x == 0) *a.dtReset = __longlong_as_double(0x7F7F7F7F7F7F7F7FLL);
+}
+
 // Tile of the TMA kernel: TE elements (box inner extent TE * sizeof >= 16 B),
 // NT threads.  TE_ = 0 picks the widest of 16/8/4 elements whose shared
 // memory stays within 72 KB (three blocks per SM); TE_ = -1 half of that,
@@ -512,6 +519,7 @@ __global__ void __launch_bounds__(NTV, (TileT<C, R, S, TEV, NTV>::MINB))
   pdl_launch_dependents();
   if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, b, e0, bar, 1);
   pdl_wait();  // the previous stage has finished: its outputs are visible
+  stage_dt_reset(a);
   if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, b, e0, bar, 2);
 
   // the global dt, fetched while the tiles are in flight
@@ -665,6 +673,7 @@ __global__ void __launch_bounds__(NT, (PipeT<C, R, S, TEV, NT, NB>::MINB))
   pdl_launch_dependents();
   if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, slot(0), blockIdx.x * TE, &bar[0], 1);
   pdl_wait();  // the previous stage has finished: its outputs are visible
+  stage_dt_reset(a);
   if (tid == 0) tma_issue_tile<C, R, S, TE>(m, nd, slot(0), blockIdx.x * TE, &bar[0], 2);
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   double dtMin = INFINITY;
@@ -887,6 +896,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
   pdl_launch_dependents();
   if (tid == 0) issue_slot(slot(0), blockIdx.x * TE, &bar[0], 1);
   pdl_wait();  // the previous stage has finished: its outputs are visible
+  stage_dt_reset(a);
   if (tid == 0) {
     issue_slot(slot(0), blockIdx.x * TE, &bar[0], 2);
     if (needUg) issue_u(slot(0), blockIdx.x * TE);
