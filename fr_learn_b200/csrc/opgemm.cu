@@ -25,12 +25,17 @@
 // warp w reads lanes 32w..32w+31 and its 32 threads store 32 consecutive
 // elements of each output point -- coalesced rows of Y.
 //
-// Split precision: x = hi + lo with hi = tf32(x) (round to nearest) and
-// lo = tf32(x - hi); Op's halves are prepared on the host, X's by the block
-// after the tile lands, elementwise and in place (hi over the landed tile, lo
-// at the same offsets of a second buffer): the swizzled positions need no
-// reordering.  D = A_hi B_hi + A_lo B_hi + A_hi B_lo; the dropped A_lo B_lo
-// term and the rounding of the lo halves are ~2^-21 relative.
+// Split precision: x = hi + lo.  The tensor core reads a TF32 operand from
+// an fp32 bit pattern with the low 13 mantissa bits dropped, so X's hi half
+// is the landed tile itself (read as trunc(x)) and its lo half is the exact
+// remainder x - trunc(x) (the same bits cleared by a mask, then a subtraction),
+// formed by the block after the tile lands, elementwise at the same offsets
+// of a second buffer: the swizzled positions need no reordering.  (Measured:
+// were the low bits rounded instead, this split would be ~2^-11 off and the
+// 1e-5 accuracy tests fail.)  Op's halves are prepared on the host: hi =
+// tf32(op) to nearest, lo = tf32(op - hi).  D = A_hi B_hi + A_lo B_hi +
+// A_hi B_lo; the dropped A_lo B_lo term and the truncation of the lo halves
+// are ~2^-20 relative.
 //
 // Persistent blocks over (128-element tile, field) pairs: one thread issues
 // the TMA loads (each tile as four [KP][32] boxes, the operator image once as
@@ -53,12 +58,6 @@
 #include "kernels_tma.cuh"
 
 namespace frg {
-
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
 
 // Shared-memory matrix descriptor (tcgen05 matrix descriptor): start,
 // leading and stride byte offsets in 16-byte units (bits 0-13, 16-29,
@@ -119,7 +118,7 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 // points; ncol: TMEM columns allocated (a power of two >= NP).  Bimg: the
 // operator image (see build_op_image).  mX: 3D map [field][K][ld] with box
 // {32, KP, 1} and the 128-byte swizzle of 32-byte chunks.  Shared memory (1024-byte aligned):
-// the landed tile (4 x [KP][32], rewritten in place as A_hi), A_lo at the same
+// the landed tile (4 x [KP][32], the A_hi operand), A_lo at the same
 // offsets, the image, two mbarriers, the TMEM address: 112 KB for a 64 x 96
 // operator, two blocks per SM.
 __global__ void __launch_bounds__(128, 1)
@@ -135,7 +134,7 @@ __global__ void __launch_bounds__(128, 1)
   }
   const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
   const uint32_t boxBytes = (uint32_t)KP * 128u;  // one [KP][32] box: the stride between 32-element groups
-  float *St = reinterpret_cast<float *>(sb);  // the landed tile, turned into A_hi in place
+  float *St = reinterpret_cast<float *>(sb);  // the landed tile: the A_hi operand
   float *Alo = reinterpret_cast<float *>(sb + aBytes);
   float *Bs = reinterpret_cast<float *>(sb + 2 * aBytes);  // hi, then lo
   const uint32_t bHalf = (uint32_t)KP * NP * 4u;
@@ -183,23 +182,19 @@ __global__ void __launch_bounds__(128, 1)
     ok = mbar_wait(&bar[0], par);
     if (__syncthreads_or(!ok)) break;
     loadsDone++;
-    // split, elementwise: the swizzle moves whole 32-byte chunks, so hi and
-    // lo keep the landed positions (the previous tile's MMAs have completed,
-    // waited below)
+    // lo halves, elementwise: the swizzle moves whole 32-byte chunks, so lo
+    // keeps the landed positions (the previous tile's MMAs have completed,
+    // waited below); the landed tile is the hi operand as it is
     {
-      float4 *S4 = reinterpret_cast<float4 *>(St), *L4 = reinterpret_cast<float4 *>(Alo);
+      const uint4 *S4 = reinterpret_cast<const uint4 *>(St);
+      float4 *L4 = reinterpret_cast<float4 *>(Alo);
       for (int i = tid; i < KP * 32; i += 128) {
-        const float4 x = S4[i];
-        float4 h, l;
-        h.x = tf32_rna(x.x);
-        h.y = tf32_rna(x.y);
-        h.z = tf32_rna(x.z);
-        h.w = tf32_rna(x.w);
-        l.x = tf32_rna(x.x - h.x);
-        l.y = tf32_rna(x.y - h.y);
-        l.z = tf32_rna(x.z - h.z);
-        l.w = tf32_rna(x.w - h.w);
-        S4[i] = h;
+        const uint4 x = S4[i];
+        float4 l;
+        l.x = __uint_as_float(x.x) - __uint_as_float(x.x & 0xFFFFE000u);
+        l.y = __uint_as_float(x.y) - __uint_as_float(x.y & 0xFFFFE000u);
+        l.z = __uint_as_float(x.z) - __uint_as_float(x.z & 0xFFFFE000u);
+        l.w = __uint_as_float(x.w) - __uint_as_float(x.w & 0xFFFFE000u);
         L4[i] = l;
       }
     }
