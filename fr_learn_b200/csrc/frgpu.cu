@@ -233,6 +233,7 @@ struct frg_solver {
   int dtLast = 0;  // slot of the dt the last step used or frg_calc_dt computed
   double *normPartial = nullptr, *normOut = nullptr, *scratchRef = nullptr;
   unsigned *err = nullptr, *ticket = nullptr;
+  unsigned *hostFlag = nullptr;  // pinned host copy of the flag word (frg_update_host)
   int curTr = 0;
   bool trValid = false, divF0Valid = false, monitor = false;
   int iter = 0, initIter = 0;
@@ -247,6 +248,7 @@ struct frg_solver {
   // tensor maps of the TMA stage kernel
   bool useTma = false;
   bool pdl = true;  // programmatic dependent launch between TMA stages (FRG_PDL=0: off)
+  bool useGraph = true;  // steps replayed from captured graphs (FRG_GRAPH=0: launched directly)
   int nSM = 0;      // multiprocessors of the device (persistent grids)
   int tmaVar = 0;  // tile-shape variant of the TMA kernel (frg_autotune)
   int nBlkTma = 0;
@@ -705,10 +707,8 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
   return FRG_OK;
 }
 
-frg_status check_flags(frg_solver *s) {
-  unsigned h = 0;
-  CK(cudaMemcpyAsync(&h, s->err, sizeof h, cudaMemcpyDeviceToHost, s->stream));
-  CK(cudaStreamSynchronize(s->stream));
+// The status of a flag word read back from the device (clears the device's).
+frg_status flags_status(frg_solver *s, unsigned h) {
   if (h) {
     CK(cudaMemsetAsync(s->err, 0, sizeof(unsigned), s->stream));
     // writeResidual's order: the dt check first (src/output.cpp:823-824), then NaN
@@ -719,6 +719,13 @@ frg_status check_flags(frg_solver *s) {
     if (h & ERRF_TIMEOUT) return fail(FRG_ERR_TIMEOUT, "a bounded device wait gave up");
   }
   return FRG_OK;
+}
+
+frg_status check_flags(frg_solver *s) {
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, s->err, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return flags_status(s, h);
 }
 
 frg_status unfused_update(frg_solver *s);
@@ -833,6 +840,7 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
       (st = dalloc(&s->normPartial, (size_t)nbDt * s->nV)) || (st = dalloc(&s->normOut, (size_t)s->nV)) ||
       (st = dalloc(&s->err, 1)) || (st = dalloc(&s->ticket, 1)))
     return st;
+  CK(cudaMallocHost(&s->hostFlag, sizeof(unsigned)));
   if (p.dtType == 0) CK(cudaMemcpy(s->dtDev, &p.dt, sizeof(double), cudaMemcpyHostToDevice));
   if (s->ks.nTma > 0 && !s->ks.grad) {
     const char *env = getenv("FRG_KERNEL");
@@ -840,6 +848,10 @@ frg_status frg_create(const frg_params *params, const frg_mesh *mesh, frg_solver
     if (s->useTma && (st = setup_tma(s.get()))) return st;
     const char *pe = getenv("FRG_PDL");
     s->pdl = !(pe && std::strcmp(pe, "0") == 0);
+  }
+  {
+    const char *ge = getenv("FRG_GRAPH");
+    s->useGraph = !(ge && std::strcmp(ge, "0") == 0);
   }
   CK(cudaDeviceGetAttribute(&s->nSM, cudaDevAttrMultiProcessorCount, dev));
   if (s->ks.vgrad) {
@@ -917,6 +929,7 @@ frg_status frg_destroy(frg_solver *s) {
   void *gp[] = {s->xvDev, s->geoTab, s->posDev, s->geoInt, s->geoFlag};
   for (void *q : gp) if (q) cudaFree(q);
   if (s->noallocOrder) cudaEventDestroy(s->noallocOrder);
+  if (s->hostFlag) cudaFreeHost(s->hostFlag);
   cudaStream_t own = s->ownStream ? s->ownStream : s->stream;  // a caller's stream is not ours to destroy
   if (own) cudaStreamDestroy(own);
   delete s;
@@ -1388,6 +1401,41 @@ static void step_done(frg_solver *s, int mode) {
   if (mode == 2) s->waveStale = false;
 }
 
+}  // extern "C"
+namespace {
+// nsteps steps of the fused path enqueued on the handle's stream (captured
+// steps replayed), without reading the flags back.
+frg_status enqueue_updates(frg_solver *s, int nsteps) {
+  frg_status st;
+  // writeResidual's check (src/output.cpp:823-824); a CFL dt is checked on
+  // the device where it is computed
+  if (nsteps > 0 && s->p.dtType == 0 && !s->grp && !(s->p.dt >= 1e-13))
+    return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
+  if ((st = ensure_traces(s))) return st;
+  for (int n = 0; n < nsteps; n++) {
+    s->iter++;
+    const int mode = dt_mode(s);
+    if (s->useGraph) {
+      cudaGraphExec_t ge;
+      if ((st = step_graph(s, mode, &ge, nullptr))) return st;
+      CK(cudaGraphLaunch(ge, s->stream));
+    } else {
+      // the same launches straight onto the stream (the bookkeeping below
+      // counts and toggles as for a replayed graph)
+      const long long before = s->launches;
+      const int ct = s->curTr;
+      if ((st = enqueue_step(s, mode))) return st;
+      s->launches = before;
+      s->curTr = ct;
+    }
+    step_done(s, mode);
+  }
+  if (nsteps > 0) s->divF0Valid = s->monitor;
+  return FRG_OK;
+}
+}  // namespace
+extern "C" {
+
 frg_status frg_update(frg_solver *s, int nsteps) {
   if (!s || nsteps < 0) return fail(FRG_ERR_ARG, "bad arguments");
   frg_status st;
@@ -1399,28 +1447,41 @@ frg_status frg_update(frg_solver *s, int nsteps) {
       if ((st = unfused_update(s))) return st;
     return check_flags(s);
   }
-  // writeResidual's check (src/output.cpp:823-824); a CFL dt is checked on
-  // the device where it is computed
-  if (nsteps > 0 && s->p.dtType == 0 && !s->grp && !(s->p.dt >= 1e-13))
-    return fail(FRG_ERR_DT, "Instability detected - dt approaching zero");
-  if ((st = ensure_traces(s))) return st;
-  for (int n = 0; n < nsteps; n++) {
-    s->iter++;
-    const int mode = dt_mode(s);
-    cudaGraphExec_t ge;
-    if ((st = step_graph(s, mode, &ge, nullptr))) return st;
-    CK(cudaGraphLaunch(ge, s->stream));
-    step_done(s, mode);
-  }
-  if (nsteps > 0) s->divF0Valid = s->monitor;
+  if ((st = enqueue_updates(s, nsteps))) return st;
   return check_flags(s);
 }
 
+// Upload, steps, download and the flag word on the handle's stream with one
+// synchronisation at the end (the host waits once per call, not after each
+// part).  The state is written back even when a flag is raised: the
+// reference's own solution array holds the failed step too when its check
+// fires (src/output.cpp:823-841).
 frg_status frg_update_host(frg_solver *s, double *U_host, int nsteps) {
-  frg_status st = frg_upload(s, FRG_U_SPTS, U_host);
-  if (st) return st;
-  if ((st = frg_update(s, nsteps))) return st;
-  return frg_download(s, FRG_U_SPTS, 0, U_host);
+  if (!s || !U_host || nsteps < 0) return fail(FRG_ERR_ARG, "bad arguments");
+  frg_status st;
+  if (s->p.timeType == 0 && s->p.dtType != 0) {  // the unfused sequence reads dt back per step
+    if ((st = frg_upload(s, FRG_U_SPTS, U_host))) return st;
+    if ((st = frg_update(s, nsteps))) return st;
+    return frg_download(s, FRG_U_SPTS, 0, U_host);
+  }
+  if ((st = ref_scratch(s, 0))) return st;
+  const size_t n = (size_t)s->nV * s->nS * s->nE;
+  CK(cudaMemcpyAsync(s->scratchRef, U_host, n * 8, cudaMemcpyHostToDevice, s->stream));
+  fr_to_device_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->scratchRef, s->U, s->nV, s->nS, s->nE,
+                                                                         s->L);
+  if ((st = post_launch(s))) return st;
+  s->trValid = false;
+  if ((st = enqueue_updates(s, nsteps))) {
+    cudaStreamSynchronize(s->stream);  // the upload still reads U_host
+    return st;
+  }
+  fr_to_ref_layout<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->U, s->scratchRef, s->nV, s->nS, s->nE,
+                                                                       s->L);
+  if ((st = post_launch(s))) return st;
+  CK(cudaMemcpyAsync(s->hostFlag, s->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(U_host, s->scratchRef, n * 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return flags_status(s, *s->hostFlag);
 }
 
 frg_status frg_residual_norm(frg_solver *s, int normType, double *out) {

@@ -264,7 +264,10 @@ frg_status frg_calc_residual_noalloc(frg_solver *s, const double *U_dev, double 
  * no host transfer.  Checks the NaN / dt flags after the last step. */
 frg_status frg_update(frg_solver *s, int nsteps);
 /* Same, with the solution in host memory ([spt][ele][field]): upload,
- * nsteps iterations, download. */
+ * nsteps iterations, download, all on the handle's stream with one host
+ * synchronisation at the end (pinned U_host keeps both copies asynchronous).
+ * U_host receives the state after the last step even when the NaN / dt check
+ * fails, as the reference's solution array does. */
 frg_status frg_update_host(frg_solver *s, double *U_host, int nsteps);
 
 /* writeResidual's norm of divF_spts[0] (normType 1, 2 or 3) of the last

@@ -69,12 +69,38 @@ def test_fixed_dt_underflow_reports_err_dt():
 
 
 def test_nan_reported_through_host_update():
-    """frg_update_host (upload, steps, download) reports the NaN too."""
+    """frg_update_host (upload, steps, download) reports the NaN too, and
+    hands back the failed step's state as the reference's array holds it."""
     mesh, ic, kw = _cases()["euler2d_tma"]
     s = Solver(mesh, dtType=0, dt=1e-3, **kw)
     s.setInitialCondition(ic)
     U = s.get("U_spts")
     U[0, 0, 3] = np.nan
+    Uh = np.ascontiguousarray(U)
     with pytest.raises(FrgError) as ei:
-        s.update_host(np.ascontiguousarray(U), 1)
+        s.update_host(Uh, 1)
     assert ei.value.code == ERR_NAN
+    assert np.isnan(Uh).any() and np.array_equal(Uh, s.get("U_spts"), equal_nan=True)
+
+
+@pytest.mark.parametrize("precision", [FRG_FP64, FRG_MIXED])
+@pytest.mark.parametrize("name,extra", [("euler2d_tma", dict(dtType=1, CFL=0.5)), ("ns3d_visc", dict(dtType=1, CFL=0.3)),
+                                        ("euler2d_tma", dict(dtType=1, CFL=0.5, timeType=0))])
+def test_host_update_matches_device_update(name, extra, precision):
+    """frg_update_host (one synchronisation per call) gives bit for bit what
+    an upload, frg_update and a download give, over consecutive calls (the
+    CFL dt carried between them); Forward Euler with CFL dt takes the
+    unfused path."""
+    mesh, ic, kw = _cases()[name]
+    a0 = 0.1 if ic == 10 else 0.0
+    a = Solver(mesh, precision=precision, **kw, **extra)
+    b = Solver(mesh, precision=precision, **kw, **extra)
+    for s in (a, b):
+        s.setInitialCondition(ic, a0)
+    Uh = np.ascontiguousarray(a.get("U_spts"))
+    for n in (1, 3, 2):
+        a.update_host(Uh, n)
+        b.set("U_spts", b.get("U_spts"))
+        b.update(n)
+        assert np.array_equal(Uh, b.get("U_spts")), n
+        assert a.time == b.time and a.dt == b.dt
