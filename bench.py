@@ -299,6 +299,24 @@ def run_gpu(args, rank, world, local_rank):
             b.synchronize()
             e2e_ms += a.elapsed_time(b)
     e2e_ms = max_over_ranks(e2e_ms, world, dev)
+    # the host link's own bound for that step: one pinned H2D and one D2H
+    # copy of the state, nothing else
+    Ud = torch.empty(Uh.shape, dtype=torch.float64, device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            Ud.copy_(Uh, non_blocking=True)
+            Uh.copy_(Ud, non_blocking=True)
+        stream.synchronize()
+        cp_ms = 0.0
+        for k in range(n_e2e):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            Ud.copy_(Uh, non_blocking=True)
+            Uh.copy_(Ud, non_blocking=True)
+            b.record(stream)
+            b.synchronize()
+            cp_ms += a.elapsed_time(b)
+    copy_ms = max_over_ranks(cp_ms, world, dev) / n_e2e
     state_bytes = s.nSpts * s.nEles * s.nFields * 8
     for sv in solvers.values():
         sv.set_stream(None)
@@ -309,7 +327,7 @@ def run_gpu(args, rank, world, local_rank):
     res["c1"] = run_advection_c1(stream)
     res["scale"] = run_scale(stream, flush)
     res["opgemm"] = run_operator_gemm(stream, flush)
-    return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes)
+    return dof, res, stage_ms, clocks, (err_l2, err_linf, rho_err, t_phys), (e2e_ms / n_e2e, state_bytes, copy_ms)
 
 
 def run_adjoint_bump(stream, nsteps=500, every=25):
@@ -1051,7 +1069,7 @@ def main():
 
         torch.distributed.init_process_group("nccl", init_method="env://",
                                              timeout=__import__("datetime").timedelta(seconds=120))
-    dof, res, stage_ms, clocks, errs, (e2e_ms, state_bytes) = run_gpu(args, rank, world, local_rank)
+    dof, res, stage_ms, clocks, errs, (e2e_ms, state_bytes, copy_ms) = run_gpu(args, rank, world, local_rank)
     if rank != 0:
         if world > 1:
             import torch
@@ -1118,7 +1136,12 @@ def main():
         "e2e": {"value": throughput(n, dof, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes,
                 "how": "frg_update_host per step: pinned host state [spt][ele][field] -> device, one RK4 step, "
-                       "state -> host"},
+                       "state -> host",
+                "host_link_bound": {"copy_ms": copy_ms, "gbs": 2 * state_bytes / (copy_ms * 1e-3) / 1e9,
+                                    "step_ms_at_bound": copy_ms + mixed["ms_per_step"],
+                                    "frac": (copy_ms + mixed["ms_per_step"]) / e2e_ms,
+                                    "how": "one pinned H2D and one D2H copy of the state (torch copies, same "
+                                           "stream), plus the device-timed step; frac = that sum / the e2e step"}},
         "adjoint": res["adjoint"],
         "ensemble": res["ensemble"],
         "taylor_green_3d": res["tgv"],

@@ -666,6 +666,7 @@ frg_status enqueue_step(frg_solver *s, int mode, cudaEvent_t *ev = nullptr) {
       vm.Acc = s->vm.Acc;
       vm.Wout = s->vm.Wout[k & 1];
       vm.trOut = s->vm.tr[s->curTr ^ 1];
+      vm.trIn = s->vm.tr[s->curTr];
       vm.JG = s->vm.JG;
       vm.det = s->vm.det;
       vm.nrm = s->vm.nrm;

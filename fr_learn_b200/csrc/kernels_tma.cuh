@@ -447,13 +447,14 @@ __device__ __forceinline__ void tma_phase_d(const OpTab<R> &op, const R *Us, S *
 // element's dt (INFINITY for other threads); in ensemble mode also reduces
 // into the element's group minimum.
 template <int NF, int TE>
-__device__ __forceinline__ double tma_tile_dt(const StageArgs &a, const double *Ws, int e0, int ln) {
+__device__ __forceinline__ double tma_tile_dt(const StageArgs &a, const double *Ws, int e0, int ln,
+                                              const double *volS = nullptr) {
   const int eg = e0 + ln;
   if (ln >= TE || eg >= a.nEle) return INFINITY;
   double iw = 0;
 #pragma unroll
   for (int f = 0; f < NF; f++) iw += Ws[f * TE + ln];
-  const double dte = a.cflFac * a.vol[eg] / iw;
+  const double dte = a.cflFac * (volS ? volS[ln] : a.vol[eg]) / iw;
   a.eleDt[eg] = dte;
   if (a.grp) {  // ensemble mode: each element into its own group's minimum
     if (!(dte > 1e-13)) atomicOr(a.err, ERRF_DT);
@@ -792,7 +793,8 @@ struct SplitT {
   }
   static constexpr int smem_bytes(int te) {
     return 2 * slot_bytes(te) + 2 * al(NV * NS * te * 8) + al(D * NV * NS * te * (int)sizeof(R)) +
-           al(NV * NF * te * (int)sizeof(R)) + al(NF * te * 8) + al((2 * NF + 1) * te * 8) + 8 * 8 + 128;
+           al(NV * NF * te * (int)sizeof(R)) + al(NF * te * 8) + al((2 * NF + 1) * te * 8) + al(2 * te * 8) + 8 * 8 +
+           128;
   }
   // the widest of 16/8/4 elements within 56 KB (four blocks per SM)
   static constexpr int TE_AUTO = smem_bytes(16) <= 56 * 1024 ? 16 : smem_bytes(8) <= 56 * 1024 ? 8 : 4;
@@ -812,7 +814,8 @@ struct SplitT {
   static constexpr int oJs = oFs + al(D * NV * NS * TE * (int)sizeof(R));
   static constexpr int oWs = oJs + al(NV * NF * TE * (int)sizeof(R));
   static constexpr int oWd = oWs + al(NF * TE * 8);
-  static constexpr int oBar = oWd + al((2 * NF + 1) * TE * 8);
+  static constexpr int oVol = oWd + al((2 * NF + 1) * TE * 8);  // double [2][TE] element volumes, by tile parity
+  static constexpr int oBar = oVol + al(2 * TE * 8);
   static constexpr int SMEM = oBar + 8 * 8 + 128;
   static_assert(SMEM == smem_bytes(TE), "layout");
   static constexpr int MINB = SMEM <= 56 * 1024 && NT <= 160 ? 4 : SMEM <= 75 * 1024 && NT <= 192 ? 3 : 2;
@@ -847,6 +850,7 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
   };
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);  // [2][3] ring groups, then U and Acc
   uint64_t *barU = bar + 6, *barA = bar + 7;
+  double *volB = reinterpret_cast<double *>(sb + T::oVol);
 
   const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x;
@@ -939,11 +943,14 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
     }
     if (__syncthreads_or(!ok)) break;
     tma_gather<C, S, TE, NT>(a, b.Nbr, b.Js, b.Wd, e0);
+    // the tile's element volumes for its ele::calcDt (one slot per tile
+    // parity: the dt is formed during the next tile)
+    if (dtn && tid < TE && e0 + tid < a.nEle) cp_async_small<8>(&volB[(j & 1) * TE + tid], &a.vol[e0 + tid]);
     tma_phase_a<C, R, S, TE, NT>(a, nd.inU, b, e0);
     // the previous tile's ele::calcDt, by the last warp, which phase A's
     // second round leaves idle; Ws is rewritten only in this tile's phase B
     if (dtn && prevE0 >= 0 && (tid >> 5) == NT / 32 - 1)
-      dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, prevE0, tid & 31));
+      dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, b.Ws, prevE0, tid & 31, &volB[((j - 1) & 1) * TE]));
     // the next tile's loads, issued by the last thread, which has one phase-A
     // item where thread 0 has two (thread 0 keeps the counts)
     if (tid == NT - 1) {
@@ -1028,7 +1035,8 @@ __global__ void __launch_bounds__(NT, (SplitT<C, R, S, TEV, NT>::MINB))
   }
   if ((flags & SF_TIME) && !a.grp && blockIdx.x == 0 && tid == 0) *a.time += dtG;
   if (dtn && (tid >> 5) == NT / 32 - 1) {
-    if (prevE0 >= 0) dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, slot(0).Ws, prevE0, tid & 31));
+    if (prevE0 >= 0)
+      dtMin = fmin(dtMin, tma_tile_dt<NF, TE>(a, slot(0).Ws, prevE0, tid & 31, &volB[((j - 1) & 1) * TE]));
     tma_dt_reduce(a, dtMin);
   }
   if (tid == 0) tma_wait_reads();

@@ -20,6 +20,8 @@
 // elements x all points x all fields), in groups on mbarriers so the later
 // groups land while the earlier phases compute; neighbour traces and
 // neighbour projected fluxes (a gather) go to shared memory with cp.async.
+// The tile's own flux-point traces are loaded too (the previous launch's
+// phase D stored them with the same sums), not recomputed.
 // Results leave through bulk tensor stores.  The stage input lands in the
 // padded point layout of the generic kernels (one empty slot after every xi
 // line, Cfg::NSP): its tensor map walks the xi line with a box one point
@@ -41,6 +43,7 @@ struct ViscMaps {
   CUtensorMap Acc;    // double 3D {L, NS, NV}: RK accumulator
   CUtensorMap Wout;   // S 3D {L, NS, NV}: next stage state
   CUtensorMap trOut;  // S 3D {L, NF, NV}: traces of the new state
+  CUtensorMap trIn;   // S 3D {L, NF, NV}: traces of the stage input (own tile; the previous launch's phase D)
   CUtensorMap JG;     // S 3D {L, NS, DIM*DIM}
   CUtensorMap det;    // S 2D {L, NS}: 1 / detJ
   CUtensorMap nrm;    // S 3D {L, NF, DIM}
@@ -109,7 +112,8 @@ struct VGradT {
   static constexpr int oDet = oJG + al(D * D * NS * TE * (int)sizeof(S));
   static constexpr int oNrm = oDet + al(NS * TE * (int)sizeof(S));  // S [D][NF][TE]
   static constexpr int oNbr = oNrm + al(D * NF * TE * (int)sizeof(S));
-  static constexpr int oBar = oNbr + al(NF * TE * 4);
+  static constexpr int oTw = oNbr + al(NF * TE * 4);  // S [NV][NF][TE] own traces of the stage input
+  static constexpr int oBar = oTw + al(NV * NF * TE * (int)sizeof(S));
   static constexpr int SMEM = oBar + 2 * 8 + 128;
   // resident blocks per SM the register budget is sized for (meshes with
   // boundary faces carry the ghost-state and wall code: two blocks)
@@ -136,7 +140,8 @@ struct VStageT {
   static constexpr int oF2 = oFn + al(NV * NF * TE * (int)sizeof(R));  // R left side's penalty projection
   static constexpr int oU0 = oF2 + al(NV * NF * TE * (int)sizeof(R));  // double [NV][NS][TE]
   static constexpr int oAcc = oU0 + al(NV * NS * TE * 8);
-  static constexpr int oBar = oAcc + al(NV * NS * TE * 8);
+  static constexpr int oTw = oAcc + al(NV * NS * TE * 8);  // S [NV][NF][TE] own traces of the stage input
+  static constexpr int oBar = oTw + al(NV * NF * TE * (int)sizeof(S));
   static constexpr int SMEM = oBar + 3 * 8 + 128;
   static constexpr int MINB = SMEM * 2 <= 227 * 1024 ? 2 : 1;
 };
@@ -211,16 +216,20 @@ __device__ __forceinline__ void visc_ghost(const StageArgs &a, int code, const R
 }
 
 // LDG common solution minus own trace at every flux point (ldg_phase with
-// the tile's normals, codes and neighbour traces in shared memory).
+// the tile's normals, codes, own traces and neighbour traces in shared
+// memory).  The own traces are the ones the previous launch's phase D (or the
+// trace kernel) stored: the same sum over the same line in the same order as
+// own_trace of the stage input, so the same values.
 template <class C, typename R, typename S, bool BC, int TE, int NT>
-__device__ __forceinline__ void visc_ldg(const StageArgs &a, const OpTab<R> &op, const R *Us, const R *Ntr,
-                                         const S *Nrm, const int *Nbr, R *Dc, int e0) {
+__device__ __forceinline__ void visc_ldg(const StageArgs &a, const S *Tw, const R *Ntr, const S *Nrm, const int *Nbr,
+                                         R *Dc, int e0) {
   constexpr int NF = C::NF, NV = C::NV, DIM = C::DIM;
   for (int it = threadIdx.x; it < NF * TE; it += NT) {
     const int f = it / TE, e = it - f * TE;
     if (e0 + e >= a.nEle) continue;
     R own[NV], oth[NV], n[DIM];
-    own_trace<C, R, TE>(op, Us, f, e, own);
+#pragma unroll
+    for (int v = 0; v < NV; v++) own[v] = (R)Tw[(v * NF + f) * TE + e];
 #pragma unroll
     for (int d = 0; d < DIM; d++) n[d] = (R)Nrm[(d * NF + f) * TE + e];
     const int code = Nbr[f * TE + e];
@@ -305,6 +314,7 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
   S *Det = reinterpret_cast<S *>(sb + T::oDet);
   S *Nrm = reinterpret_cast<S *>(sb + T::oNrm);
   int *Nbr = reinterpret_cast<int *>(sb + T::oNbr);
+  S *Tw = reinterpret_cast<S *>(sb + T::oTw);
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);
   S *FvO = reinterpret_cast<S *>(Dc);   // output after the gradient has read Dc
   S *Fv2 = reinterpret_cast<S *>(Ntr);  // penalty projection after the LDG phase has read Ntr
@@ -328,11 +338,13 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
   if (tid == 0) {
     tma_wait_reads();  // the previous tile's stores have read shared memory
     const uint32_t bst = inU ? (uint32_t)(NV * NS * TE * 8) : (uint32_t)(NV * NSP * TE * sizeof(S));
-    mbar_expect_tx(&bar[0], bst + (uint32_t)((nbr_by_tma<TE>() ? NF * TE * 4 : 0) + DIM * NF * TE * sizeof(S)));
+    mbar_expect_tx(&bar[0], bst + (uint32_t)((nbr_by_tma<TE>() ? NF * TE * 4 : 0) +
+                                             (DIM * NF * TE + NV * NF * TE) * sizeof(S)));
     if (inU) tma_load3d(Stg, &m.Uin, e0, 0, 0, &bar[0]);
     else tma_load4d(Us, &m.Uin, e0, 0, 0, 0, &bar[0]);
     if constexpr (nbr_by_tma<TE>()) tma_load2d(Nbr, &m.nbr, e0, 0, &bar[0]);
     tma_load3d(Nrm, &m.nrm, e0, 0, 0, &bar[0]);
+    tma_load3d(Tw, &m.trIn, e0, 0, 0, &bar[0]);
     mbar_expect_tx(&bar[1], (uint32_t)((DIM * DIM * NS * TE + NS * TE) * sizeof(S)));
     tma_load3d(JG, &m.JG, e0, 0, 0, &bar[1]);
     tma_load2d(Det, &m.det, e0, 0, &bar[1]);
@@ -343,6 +355,7 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
       else tma_prefetch4d(&m.Uin, en, 0, 0, 0);
       if constexpr (nbr_by_tma<TE>()) tma_prefetch2d(&m.nbr, en, 0);
       tma_prefetch3d(&m.nrm, en, 0, 0);
+      tma_prefetch3d(&m.trIn, en, 0, 0);
       tma_prefetch3d(&m.JG, en, 0, 0);
       tma_prefetch2d(&m.det, en, 0);
     }
@@ -354,7 +367,7 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
   if (inU) visc_convert_input<C, R, TE, NT>(Stg, Us);
   cp_async_wait_all();
   __syncthreads();
-  visc_ldg<C, R, S, BC, TE, NT>(a, op, Us, Ntr, Nrm, Nbr, Dc, e0);
+  visc_ldg<C, R, S, BC, TE, NT>(a, Tw, Ntr, Nrm, Nbr, Dc, e0);
   ok = mbar_wait(&bar[1], par);
   if (__syncthreads_or(!ok)) goto timeout;
   // corrected gradient at the solution points (calcGradU_spts, correctGradU)
@@ -373,7 +386,8 @@ __global__ void __launch_bounds__(NT, (VGradT<C, R, S, TE, NT>::minb(BC)))
     const int f = it / TE, e = it - f * TE;
     if (e0 + e >= a.nEle) continue;
     R u[NV], g[DIM * NV], n[DIM], Fv[DIM][NV];
-    own_trace<C, R, TE>(op, Us, f, e, u);
+#pragma unroll
+    for (int v = 0; v < NV; v++) u[v] = (R)Tw[(v * NF + f) * TE + e];
     own_grad_trace<C, R, TE>(op, dU, f, e, g);
 #pragma unroll
     for (int d = 0; d < DIM; d++) n[d] = (R)Nrm[(d * NF + f) * TE + e];
@@ -463,6 +477,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   R *F2 = reinterpret_cast<R *>(sb + T::oF2);
   double *U0 = reinterpret_cast<double *>(sb + T::oU0);
   double *Acc = reinterpret_cast<double *>(sb + T::oAcc);
+  S *Tw = reinterpret_cast<S *>(sb + T::oTw);
   uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);
   R *Js = Dc;                             // jumps, after the gradient has read Dc
   S *Wst = reinterpret_cast<S *>(JG);     // new stage state, after the fluxes have read JG
@@ -490,11 +505,12 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
     tma_wait_reads();  // the previous tile's stores have read shared memory
     const uint32_t bst = nd.inU ? (uint32_t)(NV * NS * TE * 8) : (uint32_t)(NV * NSP * TE * sizeof(S));
     mbar_expect_tx(&bar[0], bst + (uint32_t)(nbr_by_tma<TE>() ? NF * TE * 4 : 0) +
-                                (uint32_t)((DIM * NF * TE + DIM * DIM * NS * TE + NS * TE) * sizeof(S)));
+                                (uint32_t)((DIM * NF * TE + DIM * DIM * NS * TE + NS * TE + NV * NF * TE) * sizeof(S)));
     if (nd.inU) tma_load3d(U0, &m.Uin, e0, 0, 0, &bar[0]);
     else tma_load4d(Us, &m.Uin, e0, 0, 0, 0, &bar[0]);
     if constexpr (nbr_by_tma<TE>()) tma_load2d(Nbr, &m.nbr, e0, 0, &bar[0]);
     tma_load3d(Nrm, &m.nrm, e0, 0, 0, &bar[0]);
+    tma_load3d(Tw, &m.trIn, e0, 0, 0, &bar[0]);
     tma_load3d(JG, &m.JG, e0, 0, 0, &bar[0]);
     tma_load2d(Det, &m.det, e0, 0, &bar[0]);
     mbar_expect_tx(&bar[1], (uint32_t)((NF * TE + NV * NF * TE) * sizeof(S)));
@@ -510,6 +526,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
       else tma_prefetch4d(&m.Uin, en, 0, 0, 0);
       if constexpr (nbr_by_tma<TE>()) tma_prefetch2d(&m.nbr, en, 0);
       tma_prefetch3d(&m.nrm, en, 0, 0);
+      tma_prefetch3d(&m.trIn, en, 0, 0);
       tma_prefetch3d(&m.JG, en, 0, 0);
       tma_prefetch2d(&m.det, en, 0);
       tma_prefetch2d(&m.dA, en, 0);
@@ -528,7 +545,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   if (nd.inU) visc_convert_input<C, R, TE, NT>(U0, Us);
   cp_async_wait_all();
   __syncthreads();
-  visc_ldg<C, R, S, BC, TE, NT>(a, op, Us, Ntr, Nrm, Nbr, Dc, e0);
+  visc_ldg<C, R, S, BC, TE, NT>(a, Tw, Ntr, Nrm, Nbr, Dc, e0);
   __syncthreads();
 
   // ---- A: gradient, inviscid + viscous flux at the solution points,
@@ -574,14 +591,10 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
     R own[NV], dis[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) {
-      R t = 0, q = 0;
+      R q = 0;
 #pragma unroll
-      for (int j = 0; j < N1; j++) {
-        const R l = op.lag[side][j];
-        t += l * Us[(v * NSP + sx<C>(s0 + j * st)) * TE + e];
-        q += l * Fs[((dir * NV + v) * NSP + sx<C>(s0 + j * st)) * TE + e];
-      }
-      own[v] = t;
+      for (int j = 0; j < N1; j++) q += op.lag[side][j] * Fs[((dir * NV + v) * NSP + sx<C>(s0 + j * st)) * TE + e];
+      own[v] = (R)Tw[(v * NF + f) * TE + e];
       dis[v] = side ? q : -q;
     }
     R n[DIM];
