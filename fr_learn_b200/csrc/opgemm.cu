@@ -37,13 +37,14 @@
 // A_hi B_lo; the dropped A_lo B_lo term and the truncation of the lo halves
 // are ~2^-20 relative.
 //
-// Persistent blocks over (128-element tile, field) pairs: one thread issues
-// the TMA loads (each tile as four [KP][32] boxes, the operator image once as
-// two bulk copies) on one mbarrier, the block splits the tile, one thread
-// issues this tile's MMAs (committed to a second mbarrier) and, once they
-// have read the tile, the next tile's loads, and all four warps drain TMEM.
-// Every wait is bounded; on expiry the block flags an error, lets its copies
-// and MMAs land (bounded again), frees its TMEM and returns.  No multicast.
+// Persistent blocks over (128-element tile, field) pairs, warp-specialised: a
+// producer warp lands tiles (four [KP][32] boxes each, the operator image once
+// as two bulk copies) in a ring of slots, four warps form the lo halves, one
+// warp issues the MMAs into two TMEM accumulators in turn, four warps drain
+// them, all coupled by mbarriers, so a tile's load, split, MMAs and drain
+// overlap the neighbouring tiles'.  Every wait is bounded; on expiry the block
+// flags an error, lets its copies and MMAs land (bounded again), frees its
+// TMEM and returns.  No multicast.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -110,85 +111,189 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 
 // Y_v = Op X_v (+ beta Y_v) over tiles of 128 elements of one field; tile t
 // covers elements [128 (t % nT), +128) of field t / nT, nT = ceil(nEle/128).
-// Persistent: block b takes tiles b, b + gridDim.x, ...; the operator image
-// is loaded once, and the next tile's TMA loads are issued as soon as the
-// current tile's MMAs have read it, so they land while the accumulator is
-// drained (and while the SM's other block computes).  KP: K padded to a
-// multiple of 8; NP: output points padded to a multiple of 16; M: real output
-// points; ncol: TMEM columns allocated (a power of two >= NP).  Bimg: the
-// operator image (see build_op_image).  mX: 3D map [field][K][ld] with box
-// {32, KP, 1} and the 128-byte swizzle of 32-byte chunks.  Shared memory (1024-byte aligned):
-// the landed tile (4 x [KP][32], the A_hi operand), A_lo at the same
-// offsets, the image, two mbarriers, the TMEM address: 112 KB for a 64 x 96
-// operator, two blocks per SM.
-__global__ void __launch_bounds__(128, 1)
+// Persistent, one block per SM (block b takes tiles b, b + gridDim.x, ...),
+// the work split by warps so that consecutive tiles overlap:
+//   warp 8     producer: the operator image once, then each tile's four TMA
+//              boxes into one of nA landing slots (a slot is reused once the
+//              MMAs that read it have completed);
+//   warps 4-7  split: the lo half of a landed tile into the lo buffer (once
+//              the previous tile's MMAs have read that buffer);
+//   warp 9     MMA: 3 x KP/8 tcgen05.mma of a split tile into one of two TMEM
+//              accumulators (once the epilogue has drained it), then commits
+//              to the accumulator's, the slot's and the lo buffer's mbarriers;
+//   warps 0-3, 10-13  epilogue: drain an accumulator and store Y (warp w
+//              reads TMEM lanes 32(w%4)..+31; warps 0-3 the first half of the
+//              columns, warps 10-13 the second).
+// While tile j is drained, tile j+1 is split and multiplied and the tiles up
+// to j+nA land.  KP: K padded to a multiple of 8; NP: output points padded to
+// a multiple of 16; M: real output points; ncol: TMEM columns per accumulator
+// (a power of two >= NP; two accumulators).  Bimg: the operator image (see
+// build_op_image).  mX: 3D map [field][K][ld] with box {32, KP, 1} and the
+// 128-byte swizzle of 32-byte chunks.  Shared memory (1024-byte aligned): nA
+// landing slots (each 4 x [KP][32], the A_hi operand as it lands), the A_lo
+// buffer, the image (hi, then lo), then the mbarriers, the TMEM address and
+// an abort word.  Every wait is bounded and warp-uniform: a wait that gives
+// up sets the abort word, every role then leaves its loop, the producer lets
+// its issued copies land and the MMA warp its issued MMAs complete (bounded
+// again), the block flags ERRF_TIMEOUT and frees its TMEM.
+constexpr int kOgThreads = 448;
+constexpr int kOgMaxSlots = 4;
+struct OgBars {
+  uint64_t full[kOgMaxSlots], slotFree[kOgMaxSlots], img, splitDone, loFree, accFull[2], accEmpty[2];
+  uint32_t tmem;
+  int abort;
+};
+constexpr int kOgBarBytes = 256;
+static_assert(sizeof(OgBars) <= kOgBarBytes, "barrier block");
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+// Bounded, warp-uniform wait for an mbarrier phase (mask: the calling lanes):
+// false when it gives up (then the abort word is set) or another role has
+// aborted.
+__device__ __forceinline__ bool og_wait(uint64_t *b, uint32_t par, volatile int *abortF, unsigned mask) {
+  for (int i = 0; i < (1 << 22); i++) {
+    const bool done = mbar_try_wait(b, par);
+    if (__all_sync(mask, done)) return true;
+    if ((i & 63) == 63 && __any_sync(mask, *abortF != 0)) return false;
+  }
+  *abortF = 1;
+  return false;
+}
+
+__global__ void __launch_bounds__(kOgThreads, 1)
     fr_op_gemm_tc_kernel(const __grid_constant__ CUtensorMap mX, const float *__restrict__ Bimg, float *Y, int KP,
-                         int NP, int M, int ncol, int ld, int nEle, int nV, float beta, unsigned *err) {
+                         int NP, int M, int ncol, int nA, int ld, int nEle, int nV, float beta, unsigned *err) {
   // the swizzled tiles need 1024-byte alignment; the dynamic shared memory
-  // starts there (checked: no slack is allocated, so that two blocks fit)
+  // starts there (checked: no slack is allocated)
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *const sb = smem_raw;
   if (smem_u32(smem_raw) & 1023u) {
     if (threadIdx.x == 0) atomicOr(err, ERRF_ALIGN);
     return;
   }
-  const uint32_t aBytes = (uint32_t)KP * 512u;  // KP points x 128 elements x 4 bytes
+  const uint32_t aBytes = (uint32_t)KP * 512u;    // KP points x 128 elements x 4 bytes
   const uint32_t boxBytes = (uint32_t)KP * 128u;  // one [KP][32] box: the stride between 32-element groups
-  float *St = reinterpret_cast<float *>(sb);  // the landed tile: the A_hi operand
-  float *Alo = reinterpret_cast<float *>(sb + aBytes);
-  float *Bs = reinterpret_cast<float *>(sb + 2 * aBytes);  // hi, then lo
   const uint32_t bHalf = (uint32_t)KP * NP * 4u;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + 2 * aBytes + 2 * bHalf);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  unsigned char *const slots = sb;  // nA x aBytes
+  float *const Alo = reinterpret_cast<float *>(sb + (size_t)nA * aBytes);
+  unsigned char *const Bs = sb + (size_t)(nA + 1) * aBytes;  // hi, then lo
+  OgBars *const sh = reinterpret_cast<OgBars *>(Bs + 2 * (size_t)bHalf);
+  volatile int *const abortF = &sh->abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nT = (nEle + 127) / 128, nTiles = nT * nV;
   if ((int)blockIdx.x >= nTiles) return;
 
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int s = 0; s < kOgMaxSlots; s++) {
+      mbar_init(&sh->full[s], 1);
+      mbar_init(&sh->slotFree[s], 1);
+    }
+    mbar_init(&sh->img, 1);
+    mbar_init(&sh->splitDone, 128);
+    mbar_init(&sh->loFree, 1);
+    for (int a = 0; a < 2; a++) {
+      mbar_init(&sh->accFull[a], 1);
+      mbar_init(&sh->accEmpty[a], 256);
+    }
+    sh->abort = 0;
     fence_mbar_init();
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(ncol)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
+                 "r"(2 * ncol)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *tslot;
+  const uint32_t tmem = sh->tmem;
 
-  // thread 0: tile t's four 32-element boxes into St
-  auto load_tile = [&](int t) {
-    for (int q = 0; q < 4; q++)
-      tma_load3d(reinterpret_cast<unsigned char *>(St) + q * boxBytes, &mX, (t % nT) * 128 + 32 * q, 0, t / nT,
-                 &bar[0]);
-  };
-  if (tid == 0) {
-    mbar_expect_tx(&bar[0], aBytes + 2u * bHalf);
-    load_tile(blockIdx.x);
-    bulk_load(Bs, Bimg, bHalf, &bar[0]);
-    bulk_load(reinterpret_cast<unsigned char *>(Bs) + bHalf, reinterpret_cast<const unsigned char *>(Bimg) + bHalf,
-              bHalf, &bar[0]);
-  }
-  const uint32_t idesc = idesc_tf32(NP);
-  bool ok = true;
-  int j = 0;
-  int loads = 1, loadsDone = 0, mmas = 0, mmasDone = 0;  // thread 0's counts of issued / completed phases
-  for (int t = blockIdx.x; t < nTiles; t += gridDim.x, j++) {
-    const uint32_t par = (uint32_t)(j & 1);
-    ok = mbar_wait(&bar[0], par);
-    if (__syncthreads_or(!ok)) break;
-    loadsDone++;
-    // lo halves, elementwise: the swizzle moves whole 32-byte chunks, so lo
-    // keeps the landed positions (the previous tile's MMAs have completed,
-    // waited below); the landed tile is the hi operand as it is
-    {
-      const uint4 *S4 = reinterpret_cast<const uint4 *>(St);
+  if (warp == 8) {
+    if (lane == 0) {
+      // ---- producer
+      int last[kOgMaxSlots];
+      for (int s = 0; s < kOgMaxSlots; s++) last[s] = -1;
+      mbar_expect_tx(&sh->img, 2u * bHalf);
+      bulk_load(Bs, Bimg, bHalf, &sh->img);
+      bulk_load(Bs + bHalf, reinterpret_cast<const unsigned char *>(Bimg) + bHalf, bHalf, &sh->img);
+      for (int j = 0;; j++) {
+        const int t = blockIdx.x + j * gridDim.x;
+        if (t >= nTiles) break;
+        const int s = j % nA;
+        // the MMAs of the tile that used this slot before have read it
+        if (j >= nA && !og_wait(&sh->slotFree[s], (uint32_t)(((j / nA) - 1) & 1), abortF, 1u)) break;
+        mbar_expect_tx(&sh->full[s], aBytes);
+        for (int q = 0; q < 4; q++)
+          tma_load3d(slots + (size_t)s * aBytes + q * boxBytes, &mX, (t % nT) * 128 + 32 * q, 0, t / nT,
+                     &sh->full[s]);
+        last[s] = j;
+      }
+      // every issued copy lands before the block may exit (bounded)
+      mbar_wait(&sh->img, 0);
+      for (int s = 0; s < kOgMaxSlots; s++)
+        if (last[s] >= 0) mbar_wait(&sh->full[s], (uint32_t)((last[s] / nA) & 1));
+    }
+    __syncwarp();
+  } else if (warp == 9) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      const uint32_t idesc = idesc_tf32(NP);
+      int lastJ = -1;
+      if (og_wait(&sh->img, 0, abortF, 1u)) {
+        for (int j = 0;; j++) {
+          const int t = blockIdx.x + j * gridDim.x;
+          if (t >= nTiles) break;
+          const int s = j % nA, acc = j & 1;
+          if (!og_wait(&sh->splitDone, (uint32_t)(j & 1), abortF, 1u)) break;
+          // the epilogue has drained this accumulator's previous tile
+          if (j >= 2 && !og_wait(&sh->accEmpty[acc], (uint32_t)(((j >> 1) - 1) & 1), abortF, 1u)) break;
+          tc_fence_after();
+          const uint32_t aHi = smem_u32(slots + (size_t)s * aBytes), aLo = smem_u32(Alo), bHi = smem_u32(Bs),
+                         bLo = bHi + bHalf;
+          const uint32_t d = tmem + (uint32_t)(acc * ncol);
+          // A (MN-major, 32-byte-chunk swizzle): K step k is rows 8k..8k+7,
+          // two 512-byte atoms of 4 rows, in every box; the boxes boxBytes
+          // apart (leading offset), 4-row groups 512 bytes apart (stride
+          // offset).  B (K-major, no swizzle): the two K halves 128 bytes
+          // apart (leading offset), 8-row groups 256 bytes apart (stride
+          // offset), NP/8 groups per K step
+          for (int k = 0; k < KP / 8; k++) {
+            const uint64_t ah = smem_desc(aHi + k * 1024, boxBytes, 512, kLayoutSW128Base32);
+            const uint64_t al = smem_desc(aLo + k * 1024, boxBytes, 512, kLayoutSW128Base32);
+            const uint64_t bh = smem_desc(bHi + k * NP * 32, 128, 256);
+            const uint64_t bl = smem_desc(bLo + k * NP * 32, 128, 256);
+            tc_mma(d, ah, bh, idesc, k > 0 ? 1u : 0u);
+            tc_mma(d, al, bh, idesc, 1u);
+            tc_mma(d, ah, bl, idesc, 1u);
+          }
+          // each commit arrives once these MMAs have completed
+          tc_commit(&sh->accFull[acc]);
+          tc_commit(&sh->slotFree[s]);
+          tc_commit(&sh->loFree);
+          lastJ = j;
+        }
+      }
+      // every issued MMA completes before TMEM is freed (bounded)
+      if (lastJ >= 0) mbar_wait(&sh->loFree, (uint32_t)(lastJ & 1));
+    }
+    __syncwarp();
+  } else if (warp >= 4 && warp < 8) {
+    // ---- split: lo halves, elementwise (the swizzle moves whole 32-byte
+    // chunks, so lo keeps the landed positions); the landed tile is the hi
+    // operand as it is
+    for (int j = 0;; j++) {
+      const int t = blockIdx.x + j * gridDim.x;
+      if (t >= nTiles) break;
+      const int s = j % nA;
+      if (!og_wait(&sh->full[s], (uint32_t)((j / nA) & 1), abortF, 0xffffffffu)) break;
+      // the previous tile's MMAs have read the lo buffer
+      if (j >= 1 && !og_wait(&sh->loFree, (uint32_t)((j - 1) & 1), abortF, 0xffffffffu)) break;
+      const uint4 *S4 = reinterpret_cast<const uint4 *>(slots + (size_t)s * aBytes);
       float4 *L4 = reinterpret_cast<float4 *>(Alo);
-      for (int i = tid; i < KP * 32; i += 128) {
+      for (int i = tid - 128; i < KP * 32; i += 128) {
         const uint4 x = S4[i];
         float4 l;
         l.x = __uint_as_float(x.x) - __uint_as_float(x.x & 0xFFFFE000u);
@@ -197,84 +302,63 @@ __global__ void __launch_bounds__(128, 1)
         l.w = __uint_as_float(x.w) - __uint_as_float(x.w & 0xFFFFE000u);
         L4[i] = l;
       }
+      fence_proxy_async();  // the lo half is visible to the MMAs
+      mbar_arrive(&sh->splitDone);
     }
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
+  } else {
+    // ---- epilogue: lane = element, columns = output points; two groups of
+    // four warps, one per half of the columns
+    const int quad = warp & 3, half = ((NP / 16 + 1) / 2) * 16;
+    const int cb = warp < 4 ? 0 : half, ce = warp < 4 ? half : NP;
+    for (int j = 0;; j++) {
+      const int t = blockIdx.x + j * gridDim.x;
+      if (t >= nTiles) break;
+      const int acc = j & 1;
+      if (!og_wait(&sh->accFull[acc], (uint32_t)((j >> 1) & 1), abortF, 0xffffffffu)) break;
       tc_fence_after();
-      const uint32_t aHi = smem_u32(St), aLo = smem_u32(Alo), bHi = smem_u32(Bs), bLo = bHi + bHalf;
-      // A (MN-major, 32-byte-chunk swizzle): K step s is rows 8s..8s+7,
-      // two 512-byte atoms of 4 rows, in every box; the boxes boxBytes apart
-      // (leading offset), 4-row groups 512 bytes apart (stride offset).  B (K-major,
-      // no swizzle): the two K halves 128 bytes apart (leading offset),
-      // 8-row groups 256 bytes apart (stride offset), NP/8 groups per K step
-      for (int s = 0; s < KP / 8; s++) {
-        const uint64_t ah = smem_desc(aHi + s * 1024, boxBytes, 512, kLayoutSW128Base32);
-        const uint64_t al = smem_desc(aLo + s * 1024, boxBytes, 512, kLayoutSW128Base32);
-        const uint64_t bh = smem_desc(bHi + s * NP * 32, 128, 256);
-        const uint64_t bl = smem_desc(bLo + s * NP * 32, 128, 256);
-        tc_mma(tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
-        tc_mma(tmem, al, bh, idesc, 1u);
-        tc_mma(tmem, ah, bl, idesc, 1u);
-      }
-      tc_commit(&bar[1]);
-      mmas++;
-    }
-    ok = mbar_wait(&bar[1], par);
-    if (__syncthreads_or(!ok)) break;
-    mmasDone++;
-    if (tid == 0) {
-      // the MMAs have read A_hi: the next tile can land in its place while
-      // the accumulator is drained
-      const int tn = t + gridDim.x;
-      if (tn < nTiles) {
-        mbar_expect_tx(&bar[0], aBytes);
-        load_tile(tn);
-        loads++;
-      }
-    }
-    tc_fence_after();
-
-    // epilogue: lane = element, columns = output points
-    const int e = (t % nT) * 128 + 32 * warp + lane, v = t / nT;
-    const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
-    for (int c0 = 0; c0 < NP; c0 += 16) {
-      uint32_t r[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(trow + (uint32_t)c0));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (e < nEle) {
-        float *y = Y + ((size_t)v * M + c0) * ld + e;
-        const int nq = min(16, M - c0);
-        if (beta == 0.f) {  // plain stores: no read of Y
+      const int e = (t % nT) * 128 + 32 * quad + lane, v = t / nT;
+      const uint32_t trow = tmem + (uint32_t)(acc * ncol) + ((uint32_t)(32 * quad) << 16);
+      // up to 64 columns in flight per wait (four 16-column loads)
+      for (int c1 = cb; c1 < ce; c1 += 64) {
+        uint32_t r[64];
 #pragma unroll
-          for (int q = 0; q < 16; q++)
-            if (q < nq) __stcs(y + (size_t)q * ld, __uint_as_float(r[q]));
-        } else {
+        for (int u = 0; u < 4; u++)
+          if (c1 + 16 * u < ce)
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];"
+                : "=r"(r[16 * u + 0]), "=r"(r[16 * u + 1]), "=r"(r[16 * u + 2]), "=r"(r[16 * u + 3]),
+                  "=r"(r[16 * u + 4]), "=r"(r[16 * u + 5]), "=r"(r[16 * u + 6]), "=r"(r[16 * u + 7]),
+                  "=r"(r[16 * u + 8]), "=r"(r[16 * u + 9]), "=r"(r[16 * u + 10]), "=r"(r[16 * u + 11]),
+                  "=r"(r[16 * u + 12]), "=r"(r[16 * u + 13]), "=r"(r[16 * u + 14]), "=r"(r[16 * u + 15])
+                : "r"(trow + (uint32_t)(c1 + 16 * u)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (e < nEle) {
+          float *y = Y + ((size_t)v * M + c1) * ld + e;
+          const int nq = min(min(64, ce - c1), M - c1);
+          if (beta == 0.f) {  // plain stores: no read of Y
 #pragma unroll
-          for (int q = 0; q < 16; q++)
-            if (q < nq) y[(size_t)q * ld] = fmaf(beta, y[(size_t)q * ld], __uint_as_float(r[q]));
+            for (int q = 0; q < 64; q++)
+              if (q < nq) __stcs(y + (size_t)q * ld, __uint_as_float(r[q]));
+          } else {
+#pragma unroll
+            for (int q = 0; q < 64; q++)
+              if (q < nq) y[(size_t)q * ld] = fmaf(beta, y[(size_t)q * ld], __uint_as_float(r[q]));
+          }
         }
       }
+      // the accumulator is free for the MMAs of tile j + 2
+      tc_fence_before();
+      mbar_arrive(&sh->accEmpty[acc]);
     }
-    // the next tile's MMAs overwrite TMEM only after every warp has read it
-    tc_fence_before();
-    __syncthreads();
-  }
-  if (!ok && tid == 0) {
-    // a bounded wait gave up: flag it and let the load / MMAs in flight
-    // finish (bounded again) before the buffers and TMEM are released
-    atomicOr(err, ERRF_TIMEOUT);
-    for (int q = loadsDone; q < loads; q++) mbar_wait(&bar[0], (uint32_t)(q & 1));
-    for (int q = mmasDone; q < mmas; q++) mbar_wait(&bar[1], (uint32_t)(q & 1));
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_free(tmem, ncol);
+  if (tid == 0 && *abortF) atomicOr(err, ERRF_TIMEOUT);
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_free(tmem, 2 * ncol);
+  }
 }
 
 // ---------------------------------------------------------------- host side
@@ -311,16 +395,30 @@ void build_op_image(const double *op, int M, int K, int KP, int NP, std::vector<
           }
 }
 
-size_t op_gemm_smem(int KP, int NP) { return (size_t)KP * 512 * 2 + (size_t)2 * KP * NP * 4 + 64; }
+// Landing slots for a KP x NP operator: as many as fit (at most kOgMaxSlots)
+// beside the lo buffer and the image; 0 when fewer than two fit.
+static int op_gemm_slots(int KP, int NP) {
+  const size_t a = (size_t)KP * 512, fixed = a + (size_t)2 * KP * NP * 4 + kOgBarBytes;
+  if (fixed + 2 * a > (size_t)227 * 1024) return 0;
+  return (int)std::min<size_t>(kOgMaxSlots, ((size_t)227 * 1024 - fixed) / a);
+}
+size_t op_gemm_smem(int KP, int NP) {
+  const int n = std::max(2, op_gemm_slots(KP, NP));
+  return (size_t)(n + 1) * KP * 512 + (size_t)2 * KP * NP * 4 + kOgBarBytes;
+}
 
 cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, int KP, int NP, int M, int ld,
                            int nEle, int nV, float beta, unsigned *err, cudaStream_t st) {
   int ncol = 32;
   while (ncol < NP) ncol <<= 1;
+  const int nA = op_gemm_slots(KP, NP);
+  if (nA < 2) return cudaErrorInvalidValue;
   size_t smem = op_gemm_smem(KP, NP);
-  // keep (blocks per SM) x (TMEM columns) within the SM's 512 columns, so a
-  // block never waits for another's allocation
-  const size_t minSmem = (size_t)(227 * 1024) / (size_t)(512 / ncol) + 1;
+  // keep (blocks per SM) x (TMEM columns of a block) within the SM's 512
+  // columns, so a block never waits for another's allocation: with at most B
+  // blocks allowed, each takes more than 1/(B+1) of the shared memory
+  const size_t allowed = (size_t)(512 / (2 * ncol));
+  const size_t minSmem = (size_t)(227 * 1024) / (allowed + 1) + 1;
   if (smem < minSmem) smem = minSmem;
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   // per device, once: the kernel's shared-memory limit and carveout, and the
@@ -347,11 +445,11 @@ cudaError_t launch_op_gemm(const CUtensorMap &mX, const float *Bimg, float *Y, i
     }
   }
   int occ = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fr_op_gemm_tc_kernel, 128, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fr_op_gemm_tc_kernel, kOgThreads, smem);
   if (e != cudaSuccess) return e;
   const int nTiles = (nEle + 127) / 128 * nV;
   const int grid = std::max(1, std::min(nTiles, nSM * std::max(occ, 1)));
-  fr_op_gemm_tc_kernel<<<grid, 128, smem, st>>>(mX, Bimg, Y, KP, NP, M, ncol, ld, nEle, nV, beta, err);
+  fr_op_gemm_tc_kernel<<<grid, kOgThreads, smem, st>>>(mX, Bimg, Y, KP, NP, M, ncol, nA, ld, nEle, nV, beta, err);
   return cudaGetLastError();
 }
 
