@@ -106,3 +106,37 @@ def test_apply_operator_rejects_bad_calls():
     Y2 = torch.zeros((5, big.nFpts, 32), dtype=torch.float32, device="cuda")
     with pytest.raises(FrgError):
         big.apply_operator(0, 0, X2.data_ptr(), Y2.data_ptr(), 32)
+
+
+@pytest.mark.parametrize("which", [0, 3])
+def test_apply_operator_many_tiles_per_block(which):
+    """A mesh large enough that every persistent block takes ~9 tiles: the
+    ring of landing slots wraps twice and both TMEM accumulators are reused
+    several times (the small meshes above give each block one tile).  300 x
+    300 quads, P = 4 (90,000 elements, 2,816 tiles of 128 elements x field),
+    plain and accumulating products."""
+    import torch
+
+    from fr_learn_b200 import FRG_MIXED, Solver, box2d
+
+    s = Solver(box2d(300, 300), order=4, precision=FRG_MIXED)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    nV, nE = s.nFields, s.nEles
+    ld = (nE + 31) // 32 * 32
+    M, K = shapes(s, which)
+    op = s.operator(which, 0)
+    g = torch.Generator().manual_seed(7 + which)
+    X = torch.randn((nV, K, ld), generator=g, dtype=torch.float32)
+    Y0 = torch.randn((nV, M, ld), generator=g, dtype=torch.float32)
+    Xn = X.numpy().astype(np.float64)[:, :, :nE]
+    base = np.einsum("mk,vke->vme", op, Xn)
+    for beta in (0.0, 1.0):
+        Xd, Yd = X.cuda(), Y0.cuda()
+        for _ in range(2):  # two launches in a row, Y reset before each
+            Yd.copy_(Y0.cuda())
+            s.apply_operator(which, 0, Xd.data_ptr(), Yd.data_ptr(), ld, beta)
+        s.sync()
+        ref = base + beta * Y0.numpy().astype(np.float64)[:, :, :nE]
+        err = np.abs(Yd.cpu().numpy().astype(np.float64)[:, :, :nE] - ref).max() / np.abs(ref).max()
+        assert err <= TOL, (which, beta, err)
+    s.set_stream(None)
