@@ -141,8 +141,9 @@ struct VStageT {
   static constexpr int oU0 = oF2 + al(NV * NF * TE * (int)sizeof(R));  // double [NV][NS][TE]
   static constexpr int oAcc = oU0 + al(NV * NS * TE * 8);
   static constexpr int oTw = oAcc + al(NV * NS * TE * 8);  // S [NV][NF][TE] own traces of the stage input
-  static constexpr int oBar = oTw + al(NV * NF * TE * (int)sizeof(S));
-  static constexpr int SMEM = oBar + 3 * 8 + 128;
+  static constexpr int oNbrB = oTw + al(NV * NF * TE * (int)sizeof(S));  // int [NF][TE]: codes of odd tiles
+  static constexpr int oBar = oNbrB + al(NF * TE * 4);
+  static constexpr int SMEM = oBar + 4 * 8 + 128;
   static constexpr int MINB = SMEM * 2 <= 227 * 1024 ? 2 : 1;
 };
 
@@ -471,17 +472,17 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   S *Det = reinterpret_cast<S *>(sb + T::oDet);
   S *Nrm = reinterpret_cast<S *>(sb + T::oNrm);
   S *DA = reinterpret_cast<S *>(sb + T::oDA);
-  int *Nbr = reinterpret_cast<int *>(sb + T::oNbr);
   S *Fo = reinterpret_cast<S *>(sb + T::oFo);
   R *Fn = reinterpret_cast<R *>(sb + T::oFn);
   R *F2 = reinterpret_cast<R *>(sb + T::oF2);
   double *U0 = reinterpret_cast<double *>(sb + T::oU0);
   double *Acc = reinterpret_cast<double *>(sb + T::oAcc);
   S *Tw = reinterpret_cast<S *>(sb + T::oTw);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);
+  int *const NbrE = reinterpret_cast<int *>(sb + T::oNbr), *const NbrO = reinterpret_cast<int *>(sb + T::oNbrB);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sb + T::oBar);  // [3]: the next tile's codes
   R *Js = Dc;                             // jumps, after the gradient has read Dc
   S *Wst = reinterpret_cast<S *>(JG);     // new stage state, after the fluxes have read JG
-  S *TrO = reinterpret_cast<S *>(Ntr);    // new traces, after phase B has read Ntr
+  S *TrO = reinterpret_cast<S *>(Dc);     // new traces, after phase C has read the jumps
   const OpTab<R> &op = stage_op<R>(a);
   const int tid = threadIdx.x, flags = a.flags, nTiles = (a.nEle + TE - 1) / TE;
   const bool last = flags & SF_LAST, first = flags & SF_FIRST, jam = flags & SF_JAMESON;
@@ -489,26 +490,39 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   const Phys &ph = a.ph;
   bool ok = true;
   uint32_t par = 0;
+  int nbrLast = -1;  // thread 0: the tile during which the last next-tile codes load was issued
 
   if (tid == 0) {
-    for (int i = 0; i < 3; i++) mbar_init(&bar[i], 1);
+    for (int i = 0; i < 4; i++) mbar_init(&bar[i], 1);
     fence_mbar_init();
   }
   __syncthreads();
   const double dtG = (a.dtLocal || a.grp) ? 0.0 : __ldg(a.dt);
   // persistent: the block walks tiles blockIdx.x, + gridDim.x, ...; each
-  // tile's inputs are prefetched into L2 one tile ahead
+  // tile's inputs are prefetched into L2 one tile ahead, and its neighbour
+  // gathers are issued during the tile before (once that tile's phase B has
+  // read its own), with the codes in two buffers by tile parity
   for (int t = blockIdx.x, j = 0; t < nTiles; t += gridDim.x, j++) {
   const int e0 = t * TE;
+  int *const Nbr = (j & 1) ? NbrO : NbrE;  // this tile's codes
   par = (uint32_t)(j & 1);
   if (tid == 0) {
     tma_wait_reads();  // the previous tile's stores have read shared memory
     const uint32_t bst = nd.inU ? (uint32_t)(NV * NS * TE * 8) : (uint32_t)(NV * NSP * TE * sizeof(S));
-    mbar_expect_tx(&bar[0], bst + (uint32_t)(nbr_by_tma<TE>() ? NF * TE * 4 : 0) +
+    mbar_expect_tx(&bar[0], bst + (uint32_t)(nbr_by_tma<TE>() && j == 0 ? NF * TE * 4 : 0) +
                                 (uint32_t)((DIM * NF * TE + DIM * DIM * NS * TE + NS * TE + NV * NF * TE) * sizeof(S)));
     if (nd.inU) tma_load3d(U0, &m.Uin, e0, 0, 0, &bar[0]);
     else tma_load4d(Us, &m.Uin, e0, 0, 0, 0, &bar[0]);
-    if constexpr (nbr_by_tma<TE>()) tma_load2d(Nbr, &m.nbr, e0, 0, &bar[0]);
+    if constexpr (nbr_by_tma<TE>()) {
+      if (j == 0) tma_load2d(Nbr, &m.nbr, e0, 0, &bar[0]);
+      // the next tile's codes, for its gathers issued after this tile's phase B
+      const int tn = t + gridDim.x;
+      if (tn < nTiles) {
+        mbar_expect_tx(&bar[3], (uint32_t)(NF * TE * 4));
+        tma_load2d((j & 1) ? NbrE : NbrO, &m.nbr, tn * TE, 0, &bar[3]);
+        nbrLast = j;
+      }
+    }
     tma_load3d(Nrm, &m.nrm, e0, 0, 0, &bar[0]);
     tma_load3d(Tw, &m.trIn, e0, 0, 0, &bar[0]);
     tma_load3d(JG, &m.JG, e0, 0, 0, &bar[0]);
@@ -535,13 +549,16 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
       if (nd.needAcc) tma_prefetch3d(&m.Acc, en, 0, 0);
     }
   }
-  if constexpr (!nbr_by_tma<TE>()) load_nbr_plain<C, TE, NT>(a, Nbr, e0);
+  if constexpr (!nbr_by_tma<TE>())
+    if (j == 0) load_nbr_plain<C, TE, NT>(a, Nbr, e0);
 
   ok = mbar_wait(&bar[0], par);
   if (__syncthreads_or(!ok)) goto timeout;
-  visc_gather<C, S, TE, NT>(a, a.trIn, Nbr, Ntr, e0);
-  visc_gather<C, S, TE, NT>(a, a.fvnIn, Nbr, Fn, e0);
-  if (a.visc2) visc_gather_left<C, S, TE, NT>(a, Nbr, F2, e0);
+  if (j == 0) {  // later tiles' gathers were issued during the tile before
+    visc_gather<C, S, TE, NT>(a, a.trIn, Nbr, Ntr, e0);
+    visc_gather<C, S, TE, NT>(a, a.fvnIn, Nbr, Fn, e0);
+    if (a.visc2) visc_gather_left<C, S, TE, NT>(a, Nbr, F2, e0);
+  }
   if (nd.inU) visc_convert_input<C, R, TE, NT>(U0, Us);
   cp_async_wait_all();
   __syncthreads();
@@ -656,6 +673,26 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
   }
   ok = mbar_wait(&bar[2], par);
   if (__syncthreads_or(!ok)) goto timeout;
+  // phase B has read the neighbour buffers: the next tile's gathers land in
+  // them while phases C and D run (each thread issues the items whose codes
+  // it loaded itself when they come by plain loads; a failed wait skips
+  // them and is caught at the next barrier)
+  {
+    const int tn = t + gridDim.x;
+    if (tn < nTiles) {
+      const int en = tn * TE;
+      int *const Nn = (j & 1) ? NbrE : NbrO;
+      bool okN = true;
+      if constexpr (nbr_by_tma<TE>()) okN = mbar_wait(&bar[3], (uint32_t)(j & 1));
+      else load_nbr_plain<C, TE, NT>(a, Nn, en);
+      if (okN) {
+        visc_gather<C, S, TE, NT>(a, a.trIn, Nn, Ntr, en);
+        visc_gather<C, S, TE, NT>(a, a.fvnIn, Nn, Fn, en);
+        if (a.visc2) visc_gather_left<C, S, TE, NT>(a, Nn, F2, en);
+      }
+      ok = okN;
+    }
+  }
 
   // ---- C: divergence + correction, the RK update (timeStepA/B) in FP64
   for (int it = tid; it < NS * TE; it += NT) {
@@ -711,7 +748,7 @@ __global__ void __launch_bounds__(NT, (VStageT<C, R, S, TE, NT>::MINB))
     }
   }
   fence_proxy_async();
-  __syncthreads();
+  if (__syncthreads_or(!ok)) goto timeout;
   if (tid == 0) {
     if (last) tma_store3d(&m.U, e0, 0, 0, U0);
     else {
@@ -745,6 +782,7 @@ timeout:
   if (tid == 0) {
     atomicOr(a.err, ERRF_TIMEOUT);
     for (int i = 0; i < 3; i++) mbar_wait(&bar[i], par);  // bounded: let copies in flight land
+    if (nbrLast >= 0) mbar_wait(&bar[3], (uint32_t)(nbrLast & 1));
     tma_wait_reads();
   }
   cp_async_wait_all();
