@@ -40,7 +40,7 @@
 // Persistent blocks over (128-element tile, field) pairs, warp-specialised: a
 // producer warp lands tiles (four [KP][32] boxes each, the operator image once
 // as two bulk copies) in a ring of slots, four warps form the lo halves, one
-// warp issues the MMAs into two TMEM accumulators in turn, four warps drain
+// warp issues the MMAs into two TMEM accumulators in turn, eight warps drain
 // them, all coupled by mbarriers, so a tile's load, split, MMAs and drain
 // overlap the neighbouring tiles'.  Every wait is bounded; on expiry the block
 // flags an error, lets its copies and MMAs land (bounded again), frees its
