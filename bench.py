@@ -203,9 +203,14 @@ def run_gpu(args, rank, world, local_rank):
         s.set_stream(stream.cuda_stream)
         s.setInitialCondition(1)
         # tile shape of the fused stage kernel, timed on this mesh (the
-        # solution is restored afterwards)
-        with torch.cuda.stream(stream):
-            res.setdefault("tile_variant", {})[name] = int(s.autotune(10)[0])
+        # solution is restored afterwards), or the one given
+        if args.tile_variants:
+            v = int(args.tile_variants.split(",")[0 if name == "mixed" else 1])
+            s.set_tile_variant(v)
+            res.setdefault("tile_variant", {})[name] = v
+        else:
+            with torch.cuda.stream(stream):
+                res.setdefault("tile_variant", {})[name] = int(s.autotune(10)[0])
         solvers[name] = s
     dof = solvers["mixed"].nEles * solvers["mixed"].nSpts * solvers["mixed"].nFields
     sampler = ClockSampler(local_rank)
@@ -1021,6 +1026,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--tile-variants", metavar="MIXED,FP64",
+                    help="stage-kernel tile variants of the headline workload instead of autotuning them "
+                         "(e.g. for a profiler launch list, whose serialisation changes the autotuner's pick)")
     args = ap.parse_args()
     if args.profile:
         return profile_run(args.profile[0], args.profile[1] if len(args.profile) > 1 else None)
