@@ -976,7 +976,8 @@ def profile_run(case, variant=None):
     """A few steps of one workload and nothing else, for profiler captures
     (`ncu ... python bench.py --profile CASE`): builds the handle, runs,
     synchronises and returns.  Cases: c2_mixed / c2_fp64 (the 2D vortex
-    workload, 4 steps; `variant` picks the stage kernel's tile shape),
+    workload, 4 steps, L2 flushed before each as in the timed region;
+    `variant` picks the stage kernel's tile shape),
     tgv_mixed / tgv_fp64 (3D Taylor-Green, 32^3 hexes, P = 3, 2 steps),
     opgemm (the tensor-core operator GEMMs over the Taylor-Green arrays:
     spts->fpts, grad_x, correction, 2 calls each)."""
@@ -984,13 +985,21 @@ def profile_run(case, variant=None):
 
     prec = FRG_FP64 if case.endswith("fp64") else FRG_MIXED
     if case.startswith("c2"):
+        import torch
+
+        # as in the timed region: L2 flushed (a 512 MiB write) before every step
+        flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
         s = Solver(c2_mesh(), precision=prec, **c2_params())
+        s.set_stream(torch.cuda.current_stream().cuda_stream)
         s.setInitialCondition(1)
         if variant is not None:
             s.set_tile_variant(int(variant))
-        s.update(4)
+        for k in range(4):
+            flush.fill_(k)
+            s.update(1)
         s.sync()
         print(case, "time", s.time)
+        s.set_stream(None)
     elif case.startswith("tgv"):
         s = Solver(tgv_mesh(), precision=prec, **tgv_params())
         s.setInitialCondition(10, TGV_MA)
@@ -1120,8 +1129,10 @@ def main():
         "fp64_density_rel_l2_vs_exact_vortex": errs[2],
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "traffic_source": "static: dram__bytes_read.sum + dram__bytes_write.sum of one stage launch "
-                                       "from the committed ncu capture (profiles/), not measured in this run",
+                     "traffic_source": "static: dram__bytes_read.sum + dram__bytes_write.sum per stage launch, the "
+                                       "mean over the four RK stages of one step, each replayed from a clean L2, from "
+                                       "the committed ncu capture of the split kernel (profiles/); not measured in "
+                                       "this run",
                      "kernel": ("fr_stage_tma_split_kernel" if tiles["mixed"] >= 10 else "fr_stage_tma_pipe_kernel"
                                 if tiles["mixed"] >= 6 else "fr_stage_tma_kernel")
                                + f" (mixed, tile variant {tiles['mixed']})", "launch_ms": st_mixed,
