@@ -100,3 +100,33 @@ def test_fullsize_mixed_within_bound_of_fp64_oracle(oracle, name):
     assert l2 < MIXED_L2_TOL, l2
     # the mixed path's CFL dt follows the FP64 one to FP32 rounding
     assert abs(g.time - t) <= 1e-5 * t
+
+
+@pytest.mark.parametrize("name", ["vortex_128x128_p4", "bump_96x32_p3"])
+def test_fullsize_2d_autotuned_tiles_match_oracle(oracle, name):
+    """The 2D configurations with the stage kernel's tile variant picked by
+    the autotuner, as the benchmark runs them (on the 128 x 128 vortex a
+    persistent kernel whose blocks walk several tiles): FP64 within 1e-12 of
+    the oracle, mixed within 1e-6 relative L2."""
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver
+
+    _, ic, a0, kw, nsteps = _configs()[name]
+    mesh, R, dts, t = _oracle_run(oracle, name)
+    for prec in (FRG_FP64, FRG_MIXED):
+        g = Solver(mesh, precision=prec, **kw)
+        g.setInitialCondition(ic, a0)
+        v, _ = g.autotune(3)
+        assert 0 <= v < g.tile_variant_count()
+        gdt = []
+        for _ in range(nsteps):
+            g.update(1)
+            gdt.append(g.dt)
+        U = g.get("U_spts")
+        if prec == FRG_FP64:
+            assert relerr(gdt, dts) < FP64_TOL, v
+            assert relerr(U, R) < FP64_TOL, v
+            assert abs(g.time - t) <= 1e-12 * t
+        else:
+            l2 = float(np.linalg.norm(U - R) / np.linalg.norm(R))
+            assert l2 < MIXED_L2_TOL, (v, l2)
+        g.close()

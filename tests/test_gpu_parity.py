@@ -283,6 +283,58 @@ def test_tile_variants_identical_and_autotune_restores(precision, case):
     assert np.array_equal(s.get("U_spts"), ref[0])
 
 
+@pytest.mark.parametrize("case", ["periodic", "bump"])
+def test_persistent_variants_multi_tile_ragged_match_oracle(oracle, case):
+    """The persistent stage kernels (ring and split variants, the ones the
+    benchmark's autotuner picks) on meshes large enough that a block walks
+    two or more tiles and the last tile is partial: the slot ring, the
+    next-tile loads, the deferred per-tile dt and the short tile.  FP64: every
+    variant bit-identical to the one-tile kernel and within 1e-12 of the
+    oracle (state, dt of every step, time); mixed: within 1e-6 relative L2 of
+    the FP64 oracle and every variant bit-identical to the one-tile kernel."""
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver, box2d, bump2d
+
+    if case == "periodic":  # 83 x 71 = 5,893 elements: 737 tiles of 8, 1,474 of 4
+        mesh, ic = box2d(83, 71, -10, 10, -10, 10, perturb=0.1, seed=31), 1
+        kw = dict(order=4, riemannType=1, dtType=1, CFL=0.5)
+    else:  # 157 x 41 = 6,437 elements, boundaries on every side
+        mesh, ic = bump2d(157, 41), 0
+        kw = dict(order=3, riemannType=1, dtType=1, CFL=0.5, uBound=0.5 * np.sqrt(1.4), pBound=1.0)
+    nsteps = 3
+    o = oracle.Oracle(oracle.params(nDims=2, **kw), mesh)
+    o.set_ic(ic)
+    dts = []
+    for _ in range(nsteps):
+        o.update(1)
+        dts.append(o.dt)
+    R, t_o = o.U().copy(), o.time
+    o.close()
+    for prec in (FRG_FP64, FRG_MIXED):
+        ref = None
+        nvar = Solver(mesh, precision=prec, **kw).tile_variant_count()
+        for v in range(nvar):
+            s = Solver(mesh, precision=prec, **kw)
+            s.set_tile_variant(v)
+            s.setInitialCondition(ic)
+            sdt = []
+            for _ in range(nsteps):
+                s.update(1)
+                sdt.append(s.dt)
+            U = s.get("U_spts")
+            if ref is None:
+                ref = (U, sdt, s.time)
+                if prec == FRG_FP64:
+                    assert relerr(sdt, dts) < FP64_TOL
+                    assert relerr(U, R) < FP64_TOL
+                    assert abs(s.time - t_o) <= 1e-12 * t_o
+                else:
+                    assert float(np.linalg.norm(U - R) / np.linalg.norm(R)) < 1e-6
+            else:
+                assert np.array_equal(U, ref[0]), f"precision {prec}, variant {v}"
+                assert sdt == ref[1] and s.time == ref[2], f"precision {prec}, variant {v}"
+            s.close()
+
+
 def test_advection_config1_full_run(oracle):
     """The first benchmark configuration in full: 2D scalar advection of a
     Gaussian on the periodic square [-5,5]^2, 32 x 32 quads, P = 3, upwind
