@@ -372,6 +372,49 @@ def _visc3_cases():
     }
 
 
+def test_visc3_tma_multi_tile_walls_match_oracle(oracle):
+    """The 3D viscous TMA passes on a walled mesh large enough that the
+    persistent stage pass walks two or three tiles per block (the next tile's
+    gathers issued during the current one, the codes by tile parity) and the
+    last tile holds one element: 11 x 11 x 13 hexes, P = 3, adiabatic and
+    isothermal no-slip walls with the LDG penalty, CFL dt.  FP64 within 1e-12
+    of the oracle (state, dt of every step, time); mixed within 1e-6 relative
+    L2."""
+    import os
+
+    from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver, box3d
+
+    mesh = box3d(11, 11, 13, (-2, -2, -1), (2, 2, 1),
+                 bcs={"zmin": "adiabatic_noslip", "zmax": "isothermal_noslip"}, perturb=0.1, seed=45)
+    kw = dict(order=3, viscous=1, mu_inf=0.01, prandtl=0.72, fixVis=1, penFact=0.3, tau=1.0, TWall=1.0,
+              RGas=1.0 / 1.4, dtType=1, CFL=0.3)
+    nsteps = 3
+    oracle.lib().orc_set_threads(os.cpu_count() or 1)
+    o = oracle.Oracle(oracle.params(nDims=3, **kw), mesh)
+    o.set_ic(1)
+    dts = []
+    for _ in range(nsteps):
+        o.update(1)
+        dts.append(o.dt)
+    R, t_o = o.U().copy(), o.time
+    o.close()
+    for prec in (FRG_FP64, FRG_MIXED):
+        g = Solver(mesh, precision=prec, **kw)
+        g.setInitialCondition(1)
+        gdt = []
+        for _ in range(nsteps):
+            g.update(1)
+            gdt.append(g.dt)
+        U = g.get("U_spts")
+        if prec == FRG_FP64:
+            assert relerr(gdt, dts) < FP64_TOL
+            assert relerr(U, R) < FP64_TOL
+            assert abs(g.time - t_o) <= 1e-12 * t_o
+        else:
+            assert float(np.linalg.norm(U - R) / np.linalg.norm(R)) < MIXED_L2_TOL
+        g.close()
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("case", list(_visc3_cases()))
 def test_visc3_tma_kernels_match_generic_kernels(monkeypatch, precision, case):
