@@ -120,3 +120,48 @@ def test_cross_order_ensemble_graph_matches_separate_updates(precision):
     for (Ua, (ta, da)), (Ub, (tb, db)) in zip(outs[0], outs[1]):
         assert np.array_equal(Ua, Ub)
         assert np.array_equal(ta, tb) and np.array_equal(da, db)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_ensemble_persistent_variants_multi_tile(precision):
+    """Ensemble mode with the persistent stage kernels on cases large enough
+    that a block walks two or three tiles, with tiles that straddle two cases
+    (each element's group takes its own dt minimum in the deferred per-tile
+    dt): every tile variant gives, case by case, the results of the case run
+    alone."""
+    from fr_learn_b200 import Solver, box2d, concat_meshes
+
+    cases = [box2d(60, 57, -10, 10, -10, 10, perturb=0.1, seed=51), box2d(53, 65, -10, 10, -10, 10, perturb=0.1, seed=52),
+             box2d(58, 61, -8, 8, -10, 10, perturb=0.1, seed=53)]
+    union, grp = concat_meshes(cases)
+    kw = dict(order=3, riemannType=1, dtType=1, CFL=0.5, precision=precision)
+    eps = [1.0, 3.0, 5.0]
+    uinf = [(0.3, 0.2), (1.0, 1.0), (-0.5, 0.4)]
+    nsteps = 4
+    alone = []
+    for k, m in enumerate(cases):
+        s = Solver(m, **kw)
+        s.set("U_spts", _vortex(s.get("pos_spts"), eps[k], uinf[k]))
+        s.update(nsteps)
+        alone.append((s.get("U_spts"), s.time, s.dt))
+        s.close()
+    nvar = Solver(union, **kw).tile_variant_count()
+    for v in range(nvar):
+        e = Solver(union, **kw)
+        e.set_tile_variant(v)
+        e.set_groups(grp, len(cases), None)
+        pos = e.get("pos_spts")
+        e.set("U_spts", np.concatenate([_vortex(pos[:, grp == k], eps[k], uinf[k]) for k in range(len(cases))],
+                                       axis=1))
+        e.update(nsteps)
+        U = e.get("U_spts")
+        t, dt = e.group_times()
+        for k, (Ua, ta, dta) in enumerate(alone):
+            Uk = U[:, grp == k]
+            if precision == 0:
+                assert np.array_equal(Uk, Ua), (v, k, relerr(Uk, Ua))
+                assert t[k] == ta and dt[k] == dta, (v, k)
+            else:
+                assert relerr(Uk, Ua) < 1e-12, (v, k)
+                assert t[k] == pytest.approx(ta, rel=1e-15) and dt[k] == pytest.approx(dta, rel=1e-15), (v, k)
+        e.close()
