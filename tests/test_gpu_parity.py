@@ -283,7 +283,7 @@ def test_tile_variants_identical_and_autotune_restores(precision, case):
     assert np.array_equal(s.get("U_spts"), ref[0])
 
 
-@pytest.mark.parametrize("case", ["periodic", "bump"])
+@pytest.mark.parametrize("case", ["periodic_p4", "periodic_p2", "periodic_p5", "bump_p3"])
 def test_persistent_variants_multi_tile_ragged_match_oracle(oracle, case):
     """The persistent stage kernels (ring and split variants, the ones the
     benchmark's autotuner picks) on meshes large enough that a block walks
@@ -294,9 +294,17 @@ def test_persistent_variants_multi_tile_ragged_match_oracle(oracle, case):
     the FP64 oracle and every variant bit-identical to the one-tile kernel."""
     from fr_learn_b200 import FRG_FP64, FRG_MIXED, Solver, box2d, bump2d
 
-    if case == "periodic":  # 83 x 71 = 5,893 elements: 737 tiles of 8, 1,474 of 4
+    # tiles of 16 (P = 2), 8 (P = 3, 4) or 4 (P = 5) elements in mixed
+    # precision, half that in FP64; 592 persistent blocks on 148 SMs
+    if case == "periodic_p4":  # 83 x 71 = 5,893 elements: 737 tiles of 8, 1,474 of 4
         mesh, ic = box2d(83, 71, -10, 10, -10, 10, perturb=0.1, seed=31), 1
         kw = dict(order=4, riemannType=1, dtType=1, CFL=0.5)
+    elif case == "periodic_p2":  # 131 x 97 = 12,707 elements: 795 tiles of 16
+        mesh, ic = box2d(131, 97, -10, 10, -10, 10, perturb=0.1, seed=32), 1
+        kw = dict(order=2, riemannType=1, dtType=1, CFL=0.5)
+    elif case == "periodic_p5":  # 5,893 elements: 1,474 tiles of 4
+        mesh, ic = box2d(83, 71, -10, 10, -10, 10, perturb=0.05, seed=33), 1
+        kw = dict(order=5, riemannType=1, dtType=1, CFL=0.3)
     else:  # 157 x 41 = 6,437 elements, boundaries on every side
         mesh, ic = bump2d(157, 41), 0
         kw = dict(order=3, riemannType=1, dtType=1, CFL=0.5, uBound=0.5 * np.sqrt(1.4), pBound=1.0)
